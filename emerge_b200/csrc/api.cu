@@ -1,0 +1,158 @@
+// api.cu -- the extern "C" boundary of libemgpu (declared in include/emgpu.h).
+#include "common.cuh"
+
+namespace emg {
+
+namespace {
+thread_local char g_err[512] = "";
+}
+
+int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+const char *last_error() { return g_err; }
+
+namespace {
+__global__ void k_probe() {}
+
+int launch_element(const ElemArgs &a, int kind, int precision, int out, cudaStream_t s) {
+  if (precision == EMG_FP64) {
+    if (kind == EMG_MAT_ISO) return launch_element_0_0(a, out, s);
+    if (kind == EMG_MAT_DIAG) return launch_element_1_0(a, out, s);
+    if (kind == EMG_MAT_FULL) return launch_element_2_0(a, out, s);
+  } else if (precision == EMG_MIXED) {
+    if (kind == EMG_MAT_ISO) return launch_element_0_1(a, out, s);
+    if (kind == EMG_MAT_DIAG) return launch_element_1_1(a, out, s);
+    if (kind == EMG_MAT_FULL) return launch_element_2_1(a, out, s);
+  } else {
+    return fail(EMG_EINVAL, "bad precision %d", precision);
+  }
+  return fail(EMG_EINVAL, "bad material kind %d", kind);
+}
+}  // namespace
+
+}  // namespace emg
+
+using namespace emg;
+
+#define EMG_VERSION 1
+
+extern "C" {
+
+int emg_version(void) { return EMG_VERSION; }
+
+const char *emg_last_error(void) { return emg::last_error(); }
+
+int emg_device_check(int device) {
+  cudaDeviceProp p;
+  CUDA_TRY(cudaGetDeviceProperties(&p, device));
+  if (p.major != 10)
+    return fail(EMG_EDEVICE, "device %d is sm_%d%d; this build targets sm_100a", device, p.major, p.minor);
+  cudaFuncAttributes fa;
+  CUDA_TRY(cudaFuncGetAttributes(&fa, k_probe));
+  return EMG_OK;
+}
+
+int emg_status_reset(int64_t *d_status, emg_stream_t stream) {
+  if (!d_status) return fail(EMG_EINVAL, "null status pointer");
+  return status_reset(d_status, S(stream));
+}
+
+int emg_status_read(const int64_t *d_status, int64_t *h_flags, int64_t *h_first_index, emg_stream_t stream) {
+  if (!d_status || !h_flags || !h_first_index) return fail(EMG_EINVAL, "null pointer");
+  int64_t h[2];
+  CUDA_TRY(cudaMemcpyAsync(h, d_status, sizeof(h), cudaMemcpyDeviceToHost, S(stream)));
+  CUDA_TRY(cudaStreamSynchronize(S(stream)));
+  *h_flags = h[0];
+  *h_first_index = h[1];
+  return EMG_OK;
+}
+
+int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tris, emg_plan *p) {
+  if (!p) return fail(EMG_EINVAL, "null plan");
+  if (n_tets < 0 || n_assy < 0 || n_edges < 0 || n_tris < 0) return fail(EMG_EINVAL, "negative size");
+  if (n_assy > n_tets) return fail(EMG_EINVAL, "n_assy (%lld) > n_tets (%lld)", (long long)n_assy, (long long)n_tets);
+  if (n_assy > (int64_t)(INT32_MAX / 400) || n_tets > INT32_MAX || 2 * (n_edges + n_tris) >= INT32_MAX)
+    return fail(EMG_ERANGE, "mesh too large for 32-bit indexing (n_assy=%lld)", (long long)n_assy);
+  memset(p, 0, sizeof(*p));
+  p->n_tets = n_tets;
+  p->n_assy = n_assy;
+  p->n_edges = n_edges;
+  p->n_tris = n_tris;
+  p->n_ent = n_edges + n_tris;
+  p->n_items = 10 * n_assy;
+  p->N = 2 * (n_edges + n_tris);
+  plan_layout(p);
+  p->workspace_bytes = plan_workspace_bytes(p);
+  return EMG_OK;
+}
+
+int emg_plan_build(emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids, void *d_plan,
+                   void *d_ws, int32_t *d_indptr, int64_t *d_status, emg_stream_t stream) {
+  if (!p || !d_plan || !d_ws || !d_indptr || !d_status) return fail(EMG_EINVAL, "null pointer");
+  if (p->n_assy > 0 && (!d_t2e || !d_t2t)) return fail(EMG_EINVAL, "null topology pointer");
+  return plan_build(p, d_t2e, d_t2t, d_tetids, d_plan, d_ws, d_indptr, d_status, S(stream));
+}
+
+int emg_plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids,
+                    void *d_plan, const int32_t *d_indptr, int32_t *d_indices, int64_t *d_status,
+                    emg_stream_t stream) {
+  if (!p || !d_plan || !d_indptr || !d_status) return fail(EMG_EINVAL, "null pointer");
+  if (p->nnz > 0 && !d_indices) return fail(EMG_EINVAL, "null indices");
+  return plan_finish(p, d_t2e, d_t2t, d_tetids, d_plan, d_indptr, d_indices, d_status, S(stream));
+}
+
+int emg_element_values(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
+                       const int32_t *d_tetids, int64_t n_assy, const emg_material *mat, int precision, int out,
+                       double ar, double ai, double br, double bi, void *d_values, int64_t *d_status,
+                       emg_stream_t stream) {
+  if (!mat || !mat->d_er) return fail(EMG_EINVAL, "material with a null er pointer");
+  if (n_assy < 0 || n_tets < 0 || n_nodes < 0) return fail(EMG_EINVAL, "negative size");
+  if (n_assy > 0 && (!d_nodes || !d_tets || !d_values)) return fail(EMG_EINVAL, "null pointer");
+  if (n_assy > (int64_t)(INT32_MAX / 400)) return fail(EMG_ERANGE, "too many tets (%lld)", (long long)n_assy);
+  if (!d_tetids && n_assy > n_tets) return fail(EMG_EINVAL, "n_assy > n_tets without tetids");
+  ElemArgs a{d_nodes, n_nodes, d_tets, n_tets, d_tetids, n_assy, mat->d_er, mat->d_ur, ar, ai, br, bi, d_values,
+             d_status};
+  return launch_element(a, mat->kind, precision, out, S(stream));
+}
+
+int emg_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_v1, const void *d_v2,
+               int precision, double ar, double ai, double br, double bi, void *d_A, int64_t *d_status,
+               emg_stream_t stream) {
+  if (!p || !d_plan || !d_indptr) return fail(EMG_EINVAL, "null pointer");
+  if (p->nnz > 0 && (!d_v1 || !d_A)) return fail(EMG_EINVAL, "null value pointer");
+  return launch_gather(p, d_plan, d_indptr, d_v1, d_v2, precision, ar, ai, br, bi, d_A, d_status, S(stream));
+}
+
+size_t emg_assemble_workspace_size(int64_t n_assy, int precision) {
+  if (n_assy < 0) return 0;
+  return (size_t)n_assy * 400 * (precision == EMG_MIXED ? 8 : 16);
+}
+
+int emg_assemble(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const double *d_nodes,
+                 int64_t n_nodes, const int32_t *d_tets, const int32_t *d_tetids, const emg_material *mat,
+                 int precision, double ar, double ai, double br, double bi, void *d_ws, size_t ws_bytes, void *d_A,
+                 int64_t *d_status, emg_stream_t stream) {
+  if (!p) return fail(EMG_EINVAL, "null plan");
+  if (p->n_assy > 0 && (!d_ws || ws_bytes < emg_assemble_workspace_size(p->n_assy, precision)))
+    return fail(EMG_EINVAL, "workspace too small: %zu < %zu", ws_bytes,
+                emg_assemble_workspace_size(p->n_assy, precision));
+  int rc = emg_element_values(d_nodes, n_nodes, d_tets, p->n_tets, d_tetids, p->n_assy, mat, precision,
+                              EMG_OUT_LINCOMB, ar, ai, br, bi, d_ws, d_status, stream);
+  if (rc) return rc;
+  return emg_gather(p, d_plan, d_indptr, d_ws, nullptr, precision, 1.0, 0.0, 0.0, 0.0, d_A, d_status, stream);
+}
+
+int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,
+                   void *d_out, int64_t out_stride, emg_stream_t stream) {
+  if (!d_K || !d_M || !h_coef || !d_out || nf < 0 || nnz < 0) return fail(EMG_EINVAL, "null pointer or bad size");
+  if (out_stride < nnz) return fail(EMG_EINVAL, "out_stride < nnz");
+  return launch_form_sweep(d_K, d_M, d_P, nnz, h_coef, nf, d_out, out_stride, S(stream));
+}
+
+}  // extern "C"

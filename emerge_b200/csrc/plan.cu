@@ -1,0 +1,395 @@
+// plan.cu -- sparsity pattern and column-gather plan of the Nedelec-2 system.
+//
+// Replaces CSCMapping.from_rowcol / precompute_csc_pattern (mth/csc_cast.py:51-160)
+// for the structured Nedelec-2 pattern: the rows of the columns of entity x
+// (edge or face) are the DoFs of every entity that shares an assembled tet
+// with x, in four sorted blocks [edges | edges+E | faces+2E | faces+2E+F]
+// (the DoF numbering of elements/nedelec2.py:65-79).
+#include "common.cuh"
+
+namespace emg {
+namespace {
+
+__global__ void k_status_reset(int64_t *st) {
+  st[0] = 0;
+  st[1] = INT64_MAX;
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan int32 counts -> int32 offsets (n + 1 entries), int64 guard
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_PER_THREAD = 4;
+constexpr int SCAN_BLOCK = SCAN_THREADS * SCAN_PER_THREAD;
+
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long *warp_sums, long long *total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  long long x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    long long s = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      long long y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    warp_sums[lane] = s;  // inclusive
+  }
+  __syncthreads();
+  long long base = (w > 0) ? warp_sums[w - 1] : 0;
+  *total = warp_sums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const int32_t *in, int64_t n, long long *bsum) {
+  __shared__ long long ws[32];
+  int64_t base = (int64_t)blockIdx.x * SCAN_BLOCK + (int64_t)threadIdx.x * SCAN_PER_THREAD;
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; ++k)
+    if (base + k < n) s += in[base + k];
+  long long tot;
+  block_exclusive_scan(s, ws, &tot);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_bsums(long long *bsum, int64_t nb) {
+  __shared__ long long ws[32];
+  long long carry = 0;
+  for (int64_t b0 = 0; b0 < nb; b0 += SCAN_THREADS) {
+    int64_t i = b0 + threadIdx.x;
+    long long v = (i < nb) ? bsum[i] : 0;
+    long long tot;
+    long long ex = block_exclusive_scan(v, ws, &tot);
+    if (i < nb) bsum[i] = carry + ex;
+    carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const int32_t *in, int64_t n, const long long *bsum,
+                                                             int32_t *out, int64_t *st) {
+  __shared__ long long ws[32];
+  int64_t base = (int64_t)blockIdx.x * SCAN_BLOCK + (int64_t)threadIdx.x * SCAN_PER_THREAD;
+  long long v[SCAN_PER_THREAD];
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    s += v[k];
+  }
+  long long tot;
+  long long ex = block_exclusive_scan(s, ws, &tot) + bsum[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+    if (base + k < n) {
+      if (ex > INT32_MAX) flag(st, EMG_ST_CAPACITY, base + k);
+      out[base + k] = (int32_t)ex;
+    }
+    ex += v[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+    long long total = bsum[gridDim.x];
+    if (total > INT32_MAX) flag(st, EMG_ST_CAPACITY, n);
+    out[n] = (int32_t)total;
+  }
+}
+
+// in and out may alias (in-place scan of counts stored in out[0..n))
+int exclusive_scan(const int32_t *in, int64_t n, int32_t *out, long long *bsum, int64_t *st, cudaStream_t s) {
+  int64_t nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  if (nb == 0) nb = 1;
+  k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, bsum);
+  k_scan_bsums<<<1, SCAN_THREADS, 0, s>>>(bsum, nb);
+  k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, bsum, out, st);
+  return launch_check("exclusive_scan");
+}
+
+size_t scan_bsum_bytes(int64_t n) { return (size_t)((n + SCAN_BLOCK - 1) / SCAN_BLOCK + 2) * sizeof(long long); }
+
+// ---------------------------------------------------------------------------
+// plan: entity -> incident (tet, slot) items and column positions
+// ---------------------------------------------------------------------------
+constexpr int MAX_ADJ = 255;  // adjacent edges (faces) per entity: uint8 positions
+
+__device__ __forceinline__ int64_t tet_of(const int32_t *tetids, int64_t ia) { return tetids ? tetids[ia] : ia; }
+
+
+__global__ void k_count_incidence(const int32_t *t2e, const int32_t *t2t, const int32_t *tetids, int64_t nT,
+                                  int64_t nA, int64_t E, int64_t F, int32_t *cnt, int64_t *st) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nA * 10) return;
+  int64_t ia = g / 10;
+  int s = (int)(g % 10);
+  int64_t it = tet_of(tetids, ia);
+  if (it < 0 || it >= nT) {
+    flag(st, EMG_ST_INDEX, ia);
+    return;
+  }
+  int64_t raw = s < 6 ? (int64_t)t2e[(int64_t)s * nT + it] : (int64_t)t2t[(int64_t)(s - 6) * nT + it];
+  if (raw < 0 || raw >= (s < 6 ? E : F)) {
+    flag(st, EMG_ST_INDEX, ia);
+    return;
+  }
+  atomicAdd(&cnt[s < 6 ? raw : E + raw], 1);
+}
+
+__global__ void k_fill_items(const int32_t *t2e, const int32_t *t2t, const int32_t *tetids, int64_t nT, int64_t nA,
+                             int64_t E, int64_t F, const int32_t *ent_ptr, int32_t *cursor, Item *items) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nA * 10) return;
+  int64_t ia = g / 10;
+  int s = (int)(g % 10);
+  int64_t it = tet_of(tetids, ia);
+  if (it < 0 || it >= nT) return;
+  int64_t raw = s < 6 ? (int64_t)t2e[(int64_t)s * nT + it] : (int64_t)t2t[(int64_t)(s - 6) * nT + it];
+  if (raw < 0 || raw >= (s < 6 ? E : F)) return;
+  int64_t x = s < 6 ? raw : E + raw;
+  int32_t p = ent_ptr[x] + atomicAdd(&cursor[x], 1);
+  Item rec;
+  rec.ia = (int32_t)ia;
+  rec.slot = (uint8_t)s;
+#pragma unroll
+  for (int k = 0; k < 10; ++k) rec.pos[k] = 0;
+  rec.pad = 0;
+  items[p] = rec;
+}
+
+// insertion sort of each entity's items by assembled tet index (deterministic order)
+__global__ void k_sort_items(const int32_t *ent_ptr, int64_t n_ent, Item *items) {
+  int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n_ent) return;
+  int32_t b = ent_ptr[x], e = ent_ptr[x + 1];
+  for (int32_t i = b + 1; i < e; ++i) {
+    Item v = items[i];
+    int32_t j = i - 1;
+    while (j >= b && items[j].ia > v.ia) {
+      items[j + 1] = items[j];
+      --j;
+    }
+    items[j + 1] = v;
+  }
+}
+
+// Warp per entity. Candidates = the 6 edges / 4 faces of every incident tet;
+// unique values counted (count pass) or ranked (fill pass) by comparison in
+// shared memory.
+constexpr int ROWS_WARPS = 4;
+constexpr int CAND_CAP = 640;   // edge candidates per entity (6 per tet) => up to 106 incident tets
+constexpr int CAND_CAP_F = 432; // face candidates (4 per tet)
+
+template <bool FILL>
+__global__ void __launch_bounds__(ROWS_WARPS * 32)
+    k_entity_rows(const int32_t *t2e, const int32_t *t2t, const int32_t *tetids, int64_t nT, int64_t E, int64_t F,
+                  const int32_t *ent_ptr, Item *items, int64_t n_ent, int32_t *col_len, uint32_t *ent_cnt,
+                  const int32_t *indptr, int32_t *indices, int64_t *st) {
+  __shared__ int32_t cand_e[ROWS_WARPS][CAND_CAP];
+  __shared__ int32_t cand_f[ROWS_WARPS][CAND_CAP_F];
+  __shared__ uint8_t first_e[ROWS_WARPS][CAND_CAP];
+  __shared__ uint8_t first_f[ROWS_WARPS][CAND_CAP_F];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int64_t x = (int64_t)blockIdx.x * ROWS_WARPS + w;
+  if (x >= n_ent) return;
+  int32_t b = ent_ptr[x], e = ent_ptr[x + 1];
+  int nitem = e - b;
+  int ne = nitem * 6, nf = nitem * 4;
+  if (ne > CAND_CAP || nf > CAND_CAP_F) {
+    if (lane == 0) flag(st, EMG_ST_CAPACITY, x);
+    return;
+  }
+  int32_t *ce = cand_e[w], *cf = cand_f[w];
+  uint8_t *fe = first_e[w], *ff = first_f[w];
+  for (int i = lane; i < ne; i += 32) {
+    int64_t it = tet_of(tetids, items[b + i / 6].ia);
+    ce[i] = t2e[(int64_t)(i % 6) * nT + it];
+  }
+  for (int i = lane; i < nf; i += 32) {
+    int64_t it = tet_of(tetids, items[b + i / 4].ia);
+    cf[i] = t2t[(int64_t)(i % 4) * nT + it];
+  }
+  __syncwarp();
+  // first occurrences -> number of distinct adjacent edges / faces
+  int ue = 0, uf = 0;
+  for (int i = lane; i < ne; i += 32) {
+    int32_t v = ce[i];
+    bool first = true;
+    for (int j = 0; j < i; ++j) first &= (ce[j] != v);
+    fe[i] = first;
+    ue += first;
+  }
+  for (int i = lane; i < nf; i += 32) {
+    int32_t v = cf[i];
+    bool first = true;
+    for (int j = 0; j < i; ++j) first &= (cf[j] != v);
+    ff[i] = first;
+    uf += first;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ue += __shfl_xor_sync(0xffffffffu, ue, o);
+    uf += __shfl_xor_sync(0xffffffffu, uf, o);
+  }
+  if (ue > MAX_ADJ || uf > MAX_ADJ) {
+    if (lane == 0) flag(st, EMG_ST_CAPACITY, x);
+    return;
+  }
+  const bool is_edge = x < E;
+  const int64_t c0 = is_edge ? x : E + x;          // 2E + (x - E)
+  const int64_t c1 = is_edge ? x + E : E + F + x;  // 2E + F + (x - E)
+  if (!FILL) {
+    if (lane == 0) {
+      int32_t L = 2 * (ue + uf);
+      col_len[c0] = L;
+      col_len[c1] = L;
+      ent_cnt[x] = (uint32_t)ue | ((uint32_t)uf << 16);
+    }
+    return;
+  }
+  __syncwarp();
+  // rank = number of distinct smaller values; rows of the four column blocks
+  const int64_t s0 = indptr[c0], s1 = indptr[c1];
+  for (int i = lane; i < ne; i += 32) {
+    int32_t v = ce[i];
+    int r = 0;
+    for (int j = 0; j < ne; ++j) r += (fe[j] && ce[j] < v) ? 1 : 0;
+    if (fe[i]) {
+      indices[s0 + r] = v;
+      indices[s0 + ue + r] = v + (int32_t)E;
+      indices[s1 + r] = v;
+      indices[s1 + ue + r] = v + (int32_t)E;
+    }
+    items[b + i / 6].pos[i % 6] = (uint8_t)r;
+  }
+  for (int i = lane; i < nf; i += 32) {
+    int32_t v = cf[i];
+    int r = 0;
+    for (int j = 0; j < nf; ++j) r += (ff[j] && cf[j] < v) ? 1 : 0;
+    if (ff[i]) {
+      int32_t r0 = v + 2 * (int32_t)E, r1 = v + 2 * (int32_t)E + (int32_t)F;
+      indices[s0 + 2 * ue + r] = r0;
+      indices[s0 + 2 * ue + uf + r] = r1;
+      indices[s1 + 2 * ue + r] = r0;
+      indices[s1 + 2 * ue + uf + r] = r1;
+    }
+    items[b + i / 4].pos[6 + i % 4] = (uint8_t)r;
+  }
+}
+
+__global__ void k_max_col(const int32_t *col_len, int64_t n, int32_t *out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int32_t m = 0;
+  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) m = max(m, col_len[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+}  // namespace
+
+int status_reset(int64_t *st, cudaStream_t s) {
+  k_status_reset<<<1, 1, 0, s>>>(st);
+  return launch_check("k_status_reset");
+}
+
+size_t plan_layout(emg_plan *p) {
+  size_t o = 0;
+  p->off_ent_ptr = o;
+  o = align_up(o + (size_t)(p->n_ent + 1) * 4, 256);
+  p->off_item = o;
+  o = align_up(o + (size_t)p->n_items * sizeof(Item), 256);
+  p->off_item_pos = p->off_item;  // positions live inside the item records
+  p->off_ent_cnt = o;
+  o = align_up(o + (size_t)p->n_ent * 4, 256);
+  p->plan_bytes = o;
+  return o;
+}
+
+// workspace: per-entity counters, per-column lengths, scan block sums, max
+size_t plan_workspace_bytes(const emg_plan *p) {
+  size_t w = 0;
+  w = align_up(w + (size_t)p->n_ent * 4, 256);
+  w = align_up(w + (size_t)(p->N + 1) * 4, 256);
+  w = align_up(w + scan_bsum_bytes(p->N > p->n_ent ? p->N : p->n_ent), 256);
+  w = align_up(w + 16, 256);
+  return w;
+}
+
+int plan_build(emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids, void *d_plan,
+               void *d_ws, int32_t *d_indptr, int64_t *d_status, cudaStream_t s) {
+  char *plan = static_cast<char *>(d_plan);
+  char *ws = static_cast<char *>(d_ws);
+  int32_t *ent_ptr = reinterpret_cast<int32_t *>(plan + p->off_ent_ptr);
+  Item *items = reinterpret_cast<Item *>(plan + p->off_item);
+  uint32_t *ent_cnt = reinterpret_cast<uint32_t *>(plan + p->off_ent_cnt);
+  size_t o = 0;
+  int32_t *cnt = reinterpret_cast<int32_t *>(ws + o);
+  o = align_up(o + (size_t)p->n_ent * 4, 256);
+  int32_t *col_len = reinterpret_cast<int32_t *>(ws + o);
+  o = align_up(o + (size_t)(p->N + 1) * 4, 256);
+  long long *bsum = reinterpret_cast<long long *>(ws + o);
+  o = align_up(o + scan_bsum_bytes(p->N > p->n_ent ? p->N : p->n_ent), 256);
+  int32_t *maxc = reinterpret_cast<int32_t *>(ws + o);
+  int rc;
+  if ((rc = status_reset(d_status, s))) return rc;
+  if (p->n_ent > 0) CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)p->n_ent * 4, s));
+  CUDA_TRY(cudaMemsetAsync(maxc, 0, 4, s));
+  const int64_t nI = p->n_items;
+  if (nI > 0) {
+    k_count_incidence<<<grid_for(nI, 256), 256, 0, s>>>(d_t2e, d_t2t, d_tetids, p->n_tets, p->n_assy, p->n_edges,
+                                                         p->n_tris, cnt, d_status);
+    if ((rc = launch_check("k_count_incidence"))) return rc;
+  }
+  if ((rc = exclusive_scan(cnt, p->n_ent, ent_ptr, bsum, d_status, s))) return rc;
+  if (p->n_ent > 0) CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)p->n_ent * 4, s));
+  if (nI > 0) {
+    k_fill_items<<<grid_for(nI, 256), 256, 0, s>>>(d_t2e, d_t2t, d_tetids, p->n_tets, p->n_assy, p->n_edges,
+                                                    p->n_tris, ent_ptr, cnt, items);
+    if ((rc = launch_check("k_fill_items"))) return rc;
+  }
+  CUDA_TRY(cudaMemsetAsync(col_len, 0, (size_t)(p->N + 1) * 4, s));
+  if (p->n_ent > 0) {
+    k_sort_items<<<grid_for(p->n_ent, 256), 256, 0, s>>>(ent_ptr, p->n_ent, items);
+    if ((rc = launch_check("k_sort_items"))) return rc;
+    k_entity_rows<false><<<grid_for(p->n_ent, ROWS_WARPS), ROWS_WARPS * 32, 0, s>>>(
+        d_t2e, d_t2t, d_tetids, p->n_tets, p->n_edges, p->n_tris, ent_ptr, items, p->n_ent, col_len, ent_cnt,
+        nullptr, nullptr, d_status);
+    if ((rc = launch_check("k_entity_rows<count>"))) return rc;
+    k_max_col<<<296, 256, 0, s>>>(col_len, p->N, maxc);
+    if ((rc = launch_check("k_max_col"))) return rc;
+  }
+  if ((rc = exclusive_scan(col_len, p->N, d_indptr, bsum, d_status, s))) return rc;
+  int32_t h_nnz = 0, h_max = 0;
+  int64_t h_st[2] = {0, 0};
+  CUDA_TRY(cudaMemcpyAsync(&h_nnz, d_indptr + p->N, 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&h_max, maxc, 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(h_st, d_status, 16, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (h_st[0])
+    return fail(EMG_EMESH, "plan build: status flags 0x%llx at index %lld", (long long)h_st[0], (long long)h_st[1]);
+  p->nnz = h_nnz;
+  p->max_col = h_max;
+  return EMG_OK;
+}
+
+int plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids,
+                void *d_plan, const int32_t *d_indptr, int32_t *d_indices, int64_t *d_status, cudaStream_t s) {
+  if (p->n_ent == 0 || p->n_assy == 0) return EMG_OK;
+  char *plan = static_cast<char *>(d_plan);
+  const int32_t *ent_ptr = reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr);
+  Item *items = reinterpret_cast<Item *>(plan + p->off_item);
+  uint32_t *ent_cnt = reinterpret_cast<uint32_t *>(plan + p->off_ent_cnt);
+  k_entity_rows<true><<<grid_for(p->n_ent, ROWS_WARPS), ROWS_WARPS * 32, 0, s>>>(
+      d_t2e, d_t2t, d_tetids, p->n_tets, p->n_edges, p->n_tris, ent_ptr, items, p->n_ent, nullptr, ent_cnt,
+      d_indptr, d_indices, d_status);
+  return launch_check("k_entity_rows<fill>");
+}
+
+}  // namespace emg

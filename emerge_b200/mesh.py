@@ -1,0 +1,177 @@
+"""Tetrahedral mesh topology and the Nedelec-2 DoF numbering (host side).
+
+This is the input definition of the assembly path. EMerge builds it from a
+gmsh mesh in ``Mesh3D._pre_update`` (mesh3d.py:706-776) and ``Nedelec2.__init__``
+(elements/nedelec2.py:44, 61-79). The rules restated here, vectorised with numpy:
+
+* edges = unique sorted node pairs, sorted lexicographically   (mesh3d.py:706-732)
+* tris  = unique sorted node triples, sorted lexicographically (mesh3d.py:706-732)
+* tet_to_edge[6, nT] with local pairs (1,2),(1,3),(1,4),(2,3),(4,2),(3,4) and
+  tet_to_tri[4, nT] with (1,2,3),(1,3,4),(1,4,2),(2,3,4) (1-based, in the tet's
+  own vertex order)                                             (mesh3d.py:760-776)
+* Nedelec2 (SECOND_MIXED_VOLAKIS, dofsets.py:114-115): n_field = 2E + 2F and
+  tet_to_field rows 0-5 = tet_to_edge, 6-11 = tet_to_edge + E,
+  12-15 = tet_to_tri + 2E, 16-19 = tet_to_tri + 2E + F   (nedelec2.py:65-79)
+
+Also here: the seeded structured box generator used for the synthetic
+workloads (Kuhn split of each hex into 6 tets, jittered interior vertices,
+every tet oriented to det > 0).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# local (0-based) vertex pairs/triples of the reference's edge/face slots
+EDGE_SLOTS = np.array([(0, 1), (0, 2), (0, 3), (1, 2), (3, 1), (2, 3)], dtype=np.int64)
+FACE_SLOTS = np.array([(0, 1, 2), (0, 2, 3), (0, 3, 1), (1, 2, 3)], dtype=np.int64)
+# dofcodes of SECOND_MIXED_VOLAKIS: edge ids [0, 2], face ids [0, 1] (dofsets.py:39,114-115)
+VOLAKIS_DOFCODES = np.array([64] * 6 + [66] * 6 + [128] * 4 + [129] * 4, dtype=np.int64)
+
+
+def _unique_rows(keys: np.ndarray):
+    """Lexicographically sorted unique rows of an int64 (n, k) array and the
+    inverse index of every input row."""
+    n, k = keys.shape
+    order = np.lexsort(keys.T[::-1])
+    sk = keys[order]
+    new = np.ones(n, dtype=bool)
+    new[1:] = np.any(sk[1:] != sk[:-1], axis=1)
+    uid = np.cumsum(new) - 1
+    inv = np.empty(n, dtype=np.int64)
+    inv[order] = uid
+    return sk[new], inv
+
+
+@dataclass
+class TetMesh:
+    """Mesh topology in the reference's layout (``Mesh3D``): nodes f8[3,nN],
+    tets i8[4,nT], edges i8[2,E], tris i8[3,F], tet_to_edge i8[6,nT],
+    tet_to_tri i8[4,nT]."""
+
+    nodes: np.ndarray
+    tets: np.ndarray
+    edges: np.ndarray = field(init=False)
+    tris: np.ndarray = field(init=False)
+    tet_to_edge: np.ndarray = field(init=False)
+    tet_to_tri: np.ndarray = field(init=False)
+
+    def __post_init__(self):
+        self.nodes = np.ascontiguousarray(self.nodes, dtype=np.float64)
+        self.tets = np.ascontiguousarray(self.tets, dtype=np.int64)
+        if self.nodes.ndim != 2 or self.nodes.shape[0] != 3:
+            raise ValueError("nodes must have shape (3, nN)")
+        if self.tets.ndim != 2 or self.tets.shape[0] != 4:
+            raise ValueError("tets must have shape (4, nT)")
+        nT = self.tets.shape[1]
+        if nT and (self.tets.min() < 0 or self.tets.max() >= self.nodes.shape[1]):
+            raise ValueError("tet node index out of range")
+        t = self.tets.T  # (nT, 4)
+        ev = np.sort(np.stack([t[:, EDGE_SLOTS[:, 0]], t[:, EDGE_SLOTS[:, 1]]], axis=-1), axis=-1)
+        edges, einv = _unique_rows(ev.reshape(-1, 2))
+        fv = np.sort(np.stack([t[:, FACE_SLOTS[:, 0]], t[:, FACE_SLOTS[:, 1]], t[:, FACE_SLOTS[:, 2]]], axis=-1), axis=-1)
+        tris, finv = _unique_rows(fv.reshape(-1, 3))
+        self.edges = np.ascontiguousarray(edges.T)
+        self.tris = np.ascontiguousarray(tris.T)
+        self.tet_to_edge = np.ascontiguousarray(einv.reshape(nT, 6).T)
+        self.tet_to_tri = np.ascontiguousarray(finv.reshape(nT, 4).T)
+
+    @property
+    def n_nodes(self) -> int:
+        return self.nodes.shape[1]
+
+    @property
+    def n_tets(self) -> int:
+        return self.tets.shape[1]
+
+    @property
+    def n_edges(self) -> int:
+        return self.edges.shape[1]
+
+    @property
+    def n_tris(self) -> int:
+        return self.tris.shape[1]
+
+
+class Nedelec2Field:
+    """The parts of the reference ``Nedelec2`` (elements/nedelec2.py:36-101)
+    that the assembly path reads: ``mesh``, ``n_field``, ``dofcodes3d``,
+    ``get_tet_to_field()``, ``ntets``. Only SECOND_MIXED_VOLAKIS is built."""
+
+    def __init__(self, mesh: TetMesh):
+        self.mesh = mesh
+        E, F = mesh.n_edges, mesh.n_tris
+        self.nedges, self.ntris, self.ntets = E, F, mesh.n_tets
+        self.n_field = 2 * E + 2 * F
+        self.dofcodes3d = VOLAKIS_DOFCODES.copy()
+        t2f = np.empty((20, mesh.n_tets), dtype=np.int64)
+        t2f[0:6] = mesh.tet_to_edge
+        t2f[6:12] = mesh.tet_to_edge + E
+        t2f[12:16] = mesh.tet_to_tri + 2 * E
+        t2f[16:20] = mesh.tet_to_tri + 2 * E + F
+        self.tet_to_field = t2f
+
+    def get_tet_to_field(self) -> np.ndarray:
+        return self.tet_to_field
+
+    @property
+    def n_tets(self) -> int:
+        return self.ntets
+
+
+def tet_signed_volumes(nodes: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    p = nodes[:, tets]  # (3, 4, nT)
+    a, b, c = p[:, 1] - p[:, 0], p[:, 2] - p[:, 0], p[:, 3] - p[:, 0]
+    return np.einsum("in,in->n", a, np.cross(b, c, axis=0)) / 6.0
+
+
+def orient_positive(nodes: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    """Swap the last two vertices of every tet whose determinant is negative
+    (gmsh emits positively oriented tets; the reference's element matrices
+    depend on the orientation, curlcurl.py:142-167)."""
+    tets = tets.copy()
+    neg = tet_signed_volumes(nodes, tets) < 0
+    tets[2, neg], tets[3, neg] = tets[3, neg].copy(), tets[2, neg].copy()
+    return tets
+
+
+# Kuhn split of the unit cube along the main diagonal (corner 0 -> corner 7);
+# corner bit 0 = +x, bit 1 = +y, bit 2 = +z.
+_KUHN = np.array([[0, 1, 3, 7], [0, 1, 5, 7], [0, 2, 3, 7], [0, 2, 6, 7], [0, 4, 5, 7], [0, 4, 6, 7]],
+                 dtype=np.int64)
+
+
+def structured_box(nx: int, ny: int, nz: int, size=(22.86e-3, 10.16e-3, 50e-3), jitter: float = 0.05,
+                   seed: int = 0, origin=(0.0, 0.0, 0.0)):
+    """Seeded jittered structured tet box: nx*ny*nz hexes, 6 Kuhn tets each.
+
+    Interior vertices move uniformly in [-jitter, +jitter] * cell size per axis;
+    boundary vertices keep the coordinate of the face they lie on. Node id
+    ``i + (nx+1)*(j + (ny+1)*k)``. Returns (nodes f8[3,nN], tets i8[4,nT]) with
+    every tet positively oriented."""
+    rng = np.random.default_rng(seed)
+    hx, hy, hz = size[0] / nx, size[1] / ny, size[2] / nz
+    i = np.arange(nx + 1)
+    j = np.arange(ny + 1)
+    k = np.arange(nz + 1)
+    K, J, I = np.meshgrid(k, j, i, indexing="ij")
+    I, J, K = I.ravel(), J.ravel(), K.ravel()
+    x = origin[0] + I * hx
+    y = origin[1] + J * hy
+    z = origin[2] + K * hz
+    if jitter:
+        d = rng.uniform(-jitter, jitter, size=(3, I.size))
+        x = x + np.where((I > 0) & (I < nx), d[0] * hx, 0.0)
+        y = y + np.where((J > 0) & (J < ny), d[1] * hy, 0.0)
+        z = z + np.where((K > 0) & (K < nz), d[2] * hz, 0.0)
+    nodes = np.stack([x, y, z]).astype(np.float64)
+    hi, hj, hk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    hi, hj, hk = hi.transpose(2, 1, 0).ravel(), hj.transpose(2, 1, 0).ravel(), hk.transpose(2, 1, 0).ravel()
+    corners = np.empty((8, hi.size), dtype=np.int64)
+    for c in range(8):
+        ci, cj, ck = hi + (c & 1), hj + ((c >> 1) & 1), hk + ((c >> 2) & 1)
+        corners[c] = ci + (nx + 1) * (cj + (ny + 1) * ck)
+    tets = corners[_KUHN.T.reshape(-1)].reshape(4, 6, hi.size).transpose(0, 2, 1).reshape(4, -1)
+    tets = orient_positive(nodes, tets)
+    return nodes, np.ascontiguousarray(tets)

@@ -1,0 +1,176 @@
+/*
+ * emgpu -- B200 (sm_100a) Nedelec-2 curl-curl assembly, C ABI.
+ *
+ * The drop-in replaces this part of EMerge (biruichen/EMerge v2.8.0):
+ *
+ *   Evec, Bvec, cscmap = tet_mass_stiffness_matrices(field, er, ur, conductor_tets, cscmap)
+ *                                              physics/microwave/assembly/curlcurl.py:222-270
+ *   A = cscmap.to_csc(Evec - Bvec * k0**2)     physics/microwave/assembly/assembler.py:494
+ *                                              mth/csc_cast.py:51-63, 65-177
+ *
+ * Conventions
+ * - Every pointer named d_* is DEVICE memory allocated by the caller (for
+ *   example a torch tensor). The library never allocates or frees caller
+ *   memory. Host pointers are named h_*.
+ * - Arrays use the reference's layouts, C-contiguous: nodes f64[3][nN],
+ *   tets i32[4][nT], tet_to_edge i32[6][nT], tet_to_tri i32[4][nT],
+ *   material tensors complex[3][3][nT] (only the entries the material kind
+ *   needs are read, see emg_material).
+ * - Complex numbers are interleaved (re, im) pairs of double (complex128) or
+ *   float (complex64).
+ * - Every function returns 0 on success or a negative EMG_E* code; the
+ *   message of the last failure in the calling thread is emg_last_error().
+ *   No C++ exception crosses this boundary. Kernels never trap: index,
+ *   orientation and capacity violations set bits in a caller-owned device
+ *   status word (int64[2]: flags, first offending index), read with
+ *   emg_status_read.
+ * - All launches are ordered on the caller's stream; functions that must
+ *   return a size synchronise that stream and say so.
+ */
+#ifndef EMGPU_H
+#define EMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *emg_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+enum {
+  EMG_OK = 0,
+  EMG_EINVAL = -1,   /* bad argument (null pointer, size, enum) */
+  EMG_ECUDA = -2,    /* a CUDA runtime call failed */
+  EMG_EMESH = -3,    /* the device status word reports a bad mesh */
+  EMG_ERANGE = -4,   /* a size exceeds what this build supports (e.g. nnz >= 2^31) */
+  EMG_EDEVICE = -5,  /* no sm_100 device / kernel image not loadable */
+};
+
+/* status flags (device status word [0]) */
+enum {
+  EMG_ST_INDEX = 1,      /* a tet/edge/tri index outside its array */
+  EMG_ST_DEGENERATE = 2, /* zero-volume / non-finite tet or repeated vertex */
+  EMG_ST_CAPACITY = 4,   /* an entity exceeds a per-column capacity limit */
+};
+
+/* material kinds: which tensor entries are read (per tet) */
+enum {
+  EMG_MAT_ISO = 0,  /* er[0][0][t] (and ur[0][0][t]) scalars; ur may be NULL = 1 */
+  EMG_MAT_DIAG = 1, /* er/ur diagonals [d][d][t]; ur may be NULL = identity */
+  EMG_MAT_FULL = 2, /* all 9 entries; ur may be NULL = identity */
+};
+
+/* element value precision */
+enum {
+  EMG_FP64 = 0,  /* plain: everything in FP64, element values complex128 */
+  EMG_MIXED = 1, /* FP64 geometry/orientation/determinant/final sum; FP32
+                    basis-product contraction and complex64 element values */
+};
+
+/* which element values a launch produces */
+enum {
+  EMG_OUT_LINCOMB = 0, /* one array: alpha*K_e + beta*M_e */
+  EMG_OUT_K = 1,       /* stiffness (the reference's "dataE") */
+  EMG_OUT_M = 2,       /* mass      (the reference's "dataB") */
+};
+
+typedef struct {
+  int kind;          /* EMG_MAT_* */
+  const void *d_er;  /* complex128 [3][3][nT] (reference layout), required */
+  const void *d_ur;  /* complex128 [3][3][nT] or NULL (identity) */
+} emg_material;
+
+/* Gather plan: the sparsity pattern of A plus the element-slot -> nonzero map
+ * of the column gather, stored in ONE caller-allocated device blob. Filled by
+ * emg_plan_init (sizes, offsets) and emg_plan_build / emg_plan_finish. */
+typedef struct {
+  int64_t n_tets;    /* tets in the mesh */
+  int64_t n_assy;    /* assembled tets (tetids length) */
+  int64_t n_edges, n_tris;
+  int64_t n_ent;     /* n_edges + n_tris: the column owners */
+  int64_t n_items;   /* 10 * n_assy (entity, tet) incidences */
+  int64_t N;         /* 2 * n_edges + 2 * n_tris */
+  int64_t nnz;       /* set by emg_plan_build */
+  int64_t max_col;   /* longest column, set by emg_plan_build */
+  size_t off_ent_ptr, off_item, off_item_pos, off_ent_cnt; /* byte offsets in the blob */
+  size_t plan_bytes;      /* blob size */
+  size_t workspace_bytes; /* scratch needed by emg_plan_build (and only it) */
+} emg_plan;
+
+int emg_version(void);
+const char *emg_last_error(void);
+
+/* Checks that `device` is an sm_100 GPU and that this library's kernels load
+ * on it. Replaces nothing in the reference (it has no GPU path). */
+int emg_device_check(int device);
+
+/* Status word helpers (d_status: int64[2] device memory). */
+int emg_status_reset(int64_t *d_status, emg_stream_t stream);
+int emg_status_read(const int64_t *d_status, int64_t *h_flags, int64_t *h_first_index, emg_stream_t stream);
+
+/* Host-only: sizes and blob offsets for a mesh. Replaces the allocation part
+ * of CSCMapping.from_rowcol (csc_cast.py:51-53). */
+int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tris, emg_plan *plan);
+
+/* Builds the entity->tet incidence lists, column lengths and indptr[N+1]
+ * (int32) on the device, then synchronises `stream` and stores nnz/max_col in
+ * *plan. Replaces precompute_csc_pattern phases 1-3 (csc_cast.py:65-126) for
+ * the structured Nedelec-2 pattern (rows of column c = DoFs of every entity
+ * sharing a tet with c's entity). d_tetids: int32[n_assy] or NULL (all tets). */
+int emg_plan_build(emg_plan *plan, const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri,
+                   const int32_t *d_tetids, void *d_plan, void *d_workspace, int32_t *d_indptr, int64_t *d_status,
+                   emg_stream_t stream);
+
+/* Writes indices[nnz] (int32, sorted within each column) and the per-slot
+ * column positions. Replaces precompute_csc_pattern phase 4 (csc_cast.py:131-160). */
+int emg_plan_finish(const emg_plan *plan, const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri,
+                    const int32_t *d_tetids, void *d_plan, const int32_t *d_indptr, int32_t *d_indices,
+                    int64_t *d_status, emg_stream_t stream);
+
+/* Element kernel: per assembled tet ia the 20x20 element block in the
+ * reference's COO layout, value[ia*400 + 20*a + b] for reference DoF slots
+ * a, b (curlcurl.py:449-455). out = EMG_OUT_K gives the reference's dataE,
+ * EMG_OUT_M its dataB, EMG_OUT_LINCOMB alpha*K_e + beta*M_e. d_values is
+ * complex128 for EMG_FP64 and complex64 for EMG_MIXED. Replaces
+ * _matrix_builder (curlcurl.py:387-456) + ned2_tet_stiff_mass (:285-380). */
+int emg_element_values(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
+                       const int32_t *d_tetids, int64_t n_assy, const emg_material *mat, int precision, int out,
+                       double alpha_re, double alpha_im, double beta_re, double beta_im, void *d_values,
+                       int64_t *d_status, emg_stream_t stream);
+
+/* Column gather + segmented sum: A[nnz] (complex128, CSC order of the plan)
+ * = sum over element slots of alpha*V1 + beta*V2, where V1 (required) and V2
+ * (optional, NULL) are element-value arrays written by emg_element_values with
+ * the same precision. Deterministic (fixed summation order), no atomics.
+ * Replaces CSCMapping.to_csc / scatter_to_csc_c16 (csc_cast.py:55-63, 162-177). */
+int emg_gather(const emg_plan *plan, const void *d_plan, const int32_t *d_indptr, const void *d_v1,
+               const void *d_v2, int precision, double alpha_re, double alpha_im, double beta_re, double beta_im,
+               void *d_A, int64_t *d_status, emg_stream_t stream);
+
+/* Bytes of element-value scratch that emg_assemble needs. */
+size_t emg_assemble_workspace_size(int64_t n_assy, int precision);
+
+/* One-call assembly of A = alpha*K + beta*M values in CSC order: element
+ * kernel into d_workspace (emg_assemble_workspace_size bytes) + gather.
+ * Replaces tet_mass_stiffness_matrices + to_csc(Evec - Bvec*k0^2)
+ * (curlcurl.py:222-270 with a cached cscmap; assembler.py:485-494). */
+int emg_assemble(const emg_plan *plan, const void *d_plan, const int32_t *d_indptr, const double *d_nodes,
+                 int64_t n_nodes, const int32_t *d_tets, const int32_t *d_tetids, const emg_material *mat,
+                 int precision, double alpha_re, double alpha_im, double beta_re, double beta_im, void *d_workspace,
+                 size_t workspace_bytes, void *d_A, int64_t *d_status, emg_stream_t stream);
+
+/* A_f = a_f*K + b_f*M (+ c_f*P) for nf frequencies, complex128 CSC values of
+ * one pattern: K, M (and P, may be NULL) read once per call. h_coef holds
+ * nf*6 doubles (a_re, a_im, b_re, b_im, c_re, c_im) per frequency; d_out
+ * points to nf arrays of nnz complex128, d_out[f] = base + f*out_stride
+ * elements. Replaces the per-frequency to_csc(Evec - Bvec*k0^2) of the cached
+ * sweep (assembler.py:472-494). */
+int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,
+                   void *d_out, int64_t out_stride, emg_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMGPU_H */

@@ -1,0 +1,190 @@
+"""CPU ORACLE wrapper -- test infrastructure, not product code.
+
+Loads ``oracle/libemoracle.so`` (plain-C restatement of the reference path,
+``oracle/nedelec_oracle.c``) with ctypes and exposes the reference's call
+surface on numpy arrays:
+
+* ``matrix_builder``   -> curlcurl.py:387-456 ``_matrix_builder``
+* ``CSCPattern``       -> csc_cast.py:29-63   ``CSCMapping`` (from_rowcol / to_csc)
+* ``tet_mass_stiffness_matrices`` -> curlcurl.py:222-270
+* ``topology_loops``   -> mesh3d.py:706-776 and nedelec2.py:61-79 restated as
+  plain Python loops (small meshes only; checks the vectorised host topology)
+
+Parity status: pinned. ``tests/test_oracle_golden.py`` checks it against the
+fixtures that ``tests/golden/make_golden.py`` produced by running the
+reference's own numba functions.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline legs use
+this module, and only as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+from scipy.sparse import csc_matrix
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libemoracle.so")
+_lib = None
+
+_p = ctypes.c_void_p
+_i64 = ctypes.c_int64
+
+
+def build() -> str:
+    """Compile the C oracle (``make -C oracle``)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.oracle_matrix_builder.restype = ctypes.c_int
+        L.oracle_matrix_builder.argtypes = [_p, _i64, _p, _i64, _p, _i64, _p, _i64, _p, _p, _p, _p, _p, _p, _i64,
+                                            _p, _p, _p, _p, ctypes.c_int]
+        L.oracle_csc_pattern.restype = _i64
+        L.oracle_csc_pattern.argtypes = [_p, _p, _i64, _i64, _p, _p, _p, _p, ctypes.c_int]
+        L.oracle_csc_indices.restype = None
+        L.oracle_csc_indices.argtypes = [_p, _p, _p, _i64, _p]
+        L.oracle_scatter_c16.restype = None
+        L.oracle_scatter_c16.argtypes = [_p, _p, _p, _p, _i64, _p, ctypes.c_int]
+        L.oracle_scatter_lincomb_c16.restype = None
+        L.oracle_scatter_lincomb_c16.argtypes = [_p, _p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_double, _p, _p, _p, _i64, _p, ctypes.c_int]
+        L.oracle_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def num_threads() -> int:
+    return lib().oracle_num_threads()
+
+
+def matrix_builder(nodes, tets, tris, edges, tet_to_field, tet_to_edge, tet_to_tri, ur, er, tetids,
+                   nthreads: int = 0):
+    """``_matrix_builder`` (curlcurl.py:387-456): returns (dataE, dataB, rows, cols)."""
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    tets = np.ascontiguousarray(tets, dtype=np.int64)
+    tris = np.ascontiguousarray(tris, dtype=np.int64)
+    edges = np.ascontiguousarray(edges, dtype=np.int64)
+    t2f = np.ascontiguousarray(tet_to_field, dtype=np.int64)
+    t2e = np.ascontiguousarray(tet_to_edge, dtype=np.int64)
+    t2t = np.ascontiguousarray(tet_to_tri, dtype=np.int64)
+    ur = np.ascontiguousarray(ur, dtype=np.complex128)
+    er = np.ascontiguousarray(er, dtype=np.complex128)
+    tetids = np.ascontiguousarray(tetids, dtype=np.int64)
+    nA = tetids.shape[0]
+    dataE = np.empty(400 * nA, dtype=np.complex128)
+    dataB = np.empty(400 * nA, dtype=np.complex128)
+    rows = np.empty(400 * nA, dtype=np.int64)
+    cols = np.empty(400 * nA, dtype=np.int64)
+    rc = lib().oracle_matrix_builder(_ptr(nodes), nodes.shape[1], _ptr(tets), tets.shape[1], _ptr(tris),
+                                     tris.shape[1], _ptr(edges), edges.shape[1], _ptr(t2f), _ptr(t2e), _ptr(t2t),
+                                     _ptr(ur), _ptr(er), _ptr(tetids), nA, _ptr(dataE), _ptr(dataB), _ptr(rows),
+                                     _ptr(cols), int(nthreads))
+    if rc != 0:
+        raise ValueError("tet id out of range")
+    return dataE, dataB, rows, cols
+
+
+class CSCPattern:
+    """``CSCMapping`` (csc_cast.py:29-63): pattern + COO-slot map."""
+
+    def __init__(self, indptr, indices, target, col_offsets, perm, N):
+        self.indptr, self.indices, self.target = indptr, indices, target
+        self.col_offsets, self.perm, self.N = col_offsets, perm, N
+        self.nnz = int(indices.shape[0])
+
+    @staticmethod
+    def from_rowcol(rows, cols, N, nthreads: int = 0) -> "CSCPattern":
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        cols = np.ascontiguousarray(cols, dtype=np.int64)
+        S = rows.shape[0]
+        col_offsets = np.empty(N + 1, dtype=np.int64)
+        perm = np.empty(S, dtype=np.int64)
+        indptr = np.empty(N + 1, dtype=np.int64)
+        target = np.empty(S, dtype=np.int64)
+        nnz = lib().oracle_csc_pattern(_ptr(rows), _ptr(cols), S, N, _ptr(col_offsets), _ptr(perm), _ptr(indptr),
+                                       _ptr(target), int(nthreads))
+        if nnz < 0:
+            raise MemoryError("oracle pattern allocation failed")
+        indices = np.empty(nnz, dtype=np.int64)
+        lib().oracle_csc_indices(_ptr(rows), _ptr(perm), _ptr(target), S, _ptr(indices))
+        return CSCPattern(indptr, indices, target, col_offsets, perm, N)
+
+    def values(self, data, nthreads: int = 0) -> np.ndarray:
+        data = np.ascontiguousarray(data, dtype=np.complex128)
+        out = np.zeros(self.nnz, dtype=np.complex128)
+        lib().oracle_scatter_c16(_ptr(data), _ptr(self.perm), _ptr(self.target), _ptr(self.col_offsets), self.N,
+                                 _ptr(out), int(nthreads))
+        return out
+
+    def values_lincomb(self, dataE, dataB, alpha, beta, nthreads: int = 0) -> np.ndarray:
+        """scatter of alpha*dataE + beta*dataB (the caller's E - k0^2 B,
+        assembler.py:494) without materialising the combination."""
+        out = np.zeros(self.nnz, dtype=np.complex128)
+        a, b = complex(alpha), complex(beta)
+        lib().oracle_scatter_lincomb_c16(_ptr(dataE), _ptr(dataB), a.real, a.imag, b.real, b.imag, _ptr(self.perm),
+                                         _ptr(self.target),
+                                         _ptr(self.col_offsets), self.N, _ptr(out), int(nthreads))
+        return out
+
+    def to_csc(self, data, nthreads: int = 0) -> csc_matrix:
+        return csc_matrix((self.values(data, nthreads), self.indices, self.indptr), shape=(self.N, self.N))
+
+
+def tet_mass_stiffness_matrices(field, er, ur, conductor_tets, cscmap=None, nthreads: int = 0):
+    """``tet_mass_stiffness_matrices`` (curlcurl.py:222-270) on the oracle."""
+    mesh = field.mesh
+    tet_assy = np.arange(mesh.tets.shape[1])
+    conductor_tets = np.asarray(conductor_tets, dtype=np.int64)
+    if conductor_tets.shape[0] > 0:
+        tet_assy = np.delete(tet_assy, conductor_tets)
+    dataE, dataB, rows, cols = matrix_builder(mesh.nodes, mesh.tets, mesh.tris, mesh.edges,
+                                              field.get_tet_to_field(), mesh.tet_to_edge, mesh.tet_to_tri, ur, er,
+                                              tet_assy, nthreads)
+    if cscmap is None:
+        cscmap = CSCPattern.from_rowcol(rows, cols, field.n_field, nthreads)
+    return dataE, dataB, cscmap
+
+
+def topology_loops(tets: np.ndarray):
+    """Mesh3D._pre_update edge/tri extraction and tet->edge/tri maps
+    (mesh3d.py:706-776), plus Nedelec2 tet_to_field (nedelec2.py:65-79),
+    restated with the reference's own Python loops. Small meshes only."""
+    edgeset, triset = set(), set()
+    for itet in range(tets.shape[1]):
+        i1, i2, i3, i4 = sorted(int(v) for v in tets[:, itet])
+        edgeset.update({(i1, i2), (i1, i3), (i1, i4), (i2, i3), (i2, i4), (i3, i4)})
+        triset.update({(i1, i2, i3), (i1, i2, i4), (i1, i3, i4), (i2, i3, i4)})
+    edges = np.array(sorted(edgeset)).T
+    tris = np.array(sorted(triset)).T
+    inv_edges = {tuple(edges[:, i].tolist()): i for i in range(edges.shape[1])}
+    inv_tris = {tuple(tris[:, i].tolist()): i for i in range(tris.shape[1])}
+    idset1 = ((1, 2), (1, 3), (1, 4), (2, 3), (4, 2), (3, 4))
+    idset2 = ((1, 2, 3), (1, 3, 4), (1, 4, 2), (2, 3, 4))
+    nT = tets.shape[1]
+    t2e = np.zeros((6, nT), dtype=np.int64)
+    t2t = np.zeros((4, nT), dtype=np.int64)
+    for itet in range(nT):
+        t = tets[:, itet]
+        t2e[:, itet] = [inv_edges[tuple(sorted((int(t[i - 1]), int(t[j - 1]))))] for i, j in idset1]
+        t2t[:, itet] = [inv_tris[tuple(sorted((int(t[i - 1]), int(t[j - 1]), int(t[k - 1]))))] for i, j, k in idset2]
+    E, F = edges.shape[1], tris.shape[1]
+    t2f = np.zeros((20, nT), dtype=np.int64)
+    for i in range(2):  # nedof = 2 (edge ids [0, 2])
+        t2f[6 * i:6 * (i + 1)] = t2e + i * E
+    for i in range(2):  # nfdof = 2 (face ids [0, 1])
+        t2f[12 + 4 * i:12 + 4 * (i + 1)] = t2t + i * F + 2 * E
+    return edges, tris, t2e, t2t, t2f

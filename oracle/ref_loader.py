@@ -1,0 +1,65 @@
+"""Loader for the reference's own numba hot-path modules (test infrastructure).
+
+This module is ORACLE / TEST INFRASTRUCTURE. It is only ever used in a
+container where the EMerge source tree is present, to generate the golden
+fixtures committed under ``tests/golden/`` (see ``tests/golden/make_golden.py``).
+Nothing in the product package, the GPU tests, ``smoke()`` or ``bench.py``
+imports it.
+
+The reference package ``emerge`` cannot be imported normally here because its
+top-level ``__init__`` pulls in gmsh / emsutil / pyvista. Its hot-path modules
+only depend on numpy, numba, scipy and loguru, so we register empty parent
+packages whose ``__path__`` points into the source tree and import the leaf
+modules directly:
+
+* ``emerge._emerge.physics.microwave.assembly.curlcurl``
+  (``_matrix_builder`` curlcurl.py:387-456, ``ned2_tet_stiff_mass`` :285-380,
+  ``tet_coefficients`` :127-214)
+* ``emerge._emerge.mth.csc_cast`` (``CSCMapping`` :29-63,
+  ``precompute_csc_pattern`` :65-160, ``scatter_to_csc_c16`` :162-177)
+* ``emerge._emerge.mth.optimized`` (``local_mapping`` :262-296, ``matinv`` :315-357)
+"""
+from __future__ import annotations
+
+import importlib
+import os
+import sys
+import tempfile
+import types
+
+DEFAULT_REF_ROOT = "/root/reference"
+
+
+def _pkg(name: str, path: str | None) -> types.ModuleType:
+    mod = types.ModuleType(name)
+    mod.__path__ = [path] if path else []
+    sys.modules[name] = mod
+    return mod
+
+
+def load_reference(ref_root: str = DEFAULT_REF_ROOT):
+    """Import the reference hot-path modules; returns a namespace with
+    ``curlcurl``, ``csc_cast``, ``optimized`` and ``ccbf``."""
+    src = os.path.join(ref_root, "src", "emerge")
+    if not os.path.isdir(src):
+        raise FileNotFoundError(f"reference source tree not found under {ref_root}")
+    # numba wants a writable cache dir; the reference tree is read-only.
+    os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "emerge_ref_numba_cache"))
+    em = os.path.join(src, "_emerge")
+    if "emerge._emerge.physics.microwave.assembly.curlcurl" not in sys.modules:
+        _pkg("emerge", src)
+        _pkg("emerge._emerge", em)
+        _pkg("emerge._emerge.mth", os.path.join(em, "mth"))
+        _pkg("emerge._emerge.compiled", os.path.join(em, "compiled"))
+        _pkg("emerge._emerge.physics", os.path.join(em, "physics"))
+        _pkg("emerge._emerge.physics.microwave", os.path.join(em, "physics", "microwave"))
+        _pkg("emerge._emerge.physics.microwave.assembly",
+             os.path.join(em, "physics", "microwave", "assembly"))
+        elements = _pkg("emerge._emerge.elements", None)
+        elements.Nedelec2 = object  # only used as a type hint by curlcurl.py:21
+    ns = types.SimpleNamespace()
+    ns.curlcurl = importlib.import_module("emerge._emerge.physics.microwave.assembly.curlcurl")
+    ns.csc_cast = importlib.import_module("emerge._emerge.mth.csc_cast")
+    ns.optimized = importlib.import_module("emerge._emerge.mth.optimized")
+    ns.ccbf = importlib.import_module("emerge._emerge.compiled.ccbf")
+    return ns

@@ -1,0 +1,36 @@
+"""libemgpu.so builds for sm_100a, loads without a GPU and exports every
+symbol include/emgpu.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+from emerge_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "emgpu.h")).read()
+    return sorted(set(re.findall(r"\b(emg_[a-z_]+)\s*\(", src)))
+
+
+def test_header_matches_binding_list():
+    assert declared_symbols() == sorted(L.EXPORTS)
+
+
+def test_library_loads_and_exports_all():
+    lib = L.lib()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    assert lib.emg_version() >= 1
+
+
+def test_host_only_entry_points():
+    lib = L.lib()
+    p = L.Plan()
+    assert lib.emg_plan_init(12960, 12960, 17004, 27144, ctypes.byref(p)) == 0
+    assert p.N == 88296 and p.n_items == 129600 and p.plan_bytes > 0 and p.workspace_bytes > 0
+    assert lib.emg_plan_init(-1, 0, 0, 0, ctypes.byref(p)) == L.EMG_EINVAL
+    assert b"negative" in lib.emg_last_error()
+    assert lib.emg_assemble_workspace_size(10, L.EMG_FP64) == 10 * 400 * 16
+    assert lib.emg_assemble_workspace_size(10, L.EMG_MIXED) == 10 * 400 * 8
