@@ -41,15 +41,18 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-tets", type=int, default=200000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default=None, help="hex grid nx,ny,nz of the dielectric box (default 100,50,67)")
+    ap.add_argument("--forms", default="fp64,mixed", help="comma list of forms to time (fp64, mixed, exact)")
     return ap.parse_args()
 
 
-def make_workload(name, seed_offset=0):
+def make_workload(name, seed_offset=0, grid=None):
     from emerge_b200 import workloads as W
 
     if name == "wr90_air":
         return W.wr90_air(seed=0 + seed_offset)
-    return W.wr90_dielectric(seed=1 + seed_offset)
+    n = tuple(int(x) for x in grid.split(",")) if grid else (100, 50, 67)
+    return W.wr90_dielectric(n=n, seed=1 + seed_offset)
 
 
 # ---------------------------------------------------------------- clocks
@@ -150,7 +153,7 @@ def run_reference(args, rank, world):
     host cores, same metric/unit/config; rank 0 only."""
     if rank != 0:
         return None
-    wl = make_workload(args.config)
+    wl = make_workload(args.config, grid=args.grid)
     cb = CpuBaseline(wl, args.cpu_sample_tets)
     for _ in range(args.warmup):
         cb.step()
@@ -236,7 +239,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     L.check(L.lib().emg_device_check(local_rank))
-    wl = make_workload(args.config, seed_offset=0)
+    wl = make_workload(args.config, seed_offset=0, grid=args.grid)
     f = wl.field
     dmesh = DeviceMesh(f, wl.conductor_tets, dev)
     t0 = time.perf_counter()
@@ -249,7 +252,9 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     out = torch.empty(cmap.nnz, dtype=torch.complex128, device=dev)
     results = {}
-    for pname, prec in (("fp64", L.EMG_FP64), ("mixed", L.EMG_MIXED)):
+    forms = {"fp64": L.EMG_FP64, "mixed": L.EMG_MIXED, "exact": L.EMG_EXACT}
+    for pname in [x for x in ("fp64", "mixed", "exact") if x in args.forms.split(",")]:
+        prec = forms[pname]
         job = _Job(dmesh, dmat, prec)
         cmap.workspace(prec)
 

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_HERE, "libemgpu.so")
 EMG_OK, EMG_EINVAL, EMG_ECUDA, EMG_EMESH, EMG_ERANGE, EMG_EDEVICE = 0, -1, -2, -3, -4, -5
 EMG_ST_INDEX, EMG_ST_DEGENERATE, EMG_ST_CAPACITY = 1, 2, 4
 EMG_MAT_ISO, EMG_MAT_DIAG, EMG_MAT_FULL = 0, 1, 2
-EMG_FP64, EMG_MIXED = 0, 1
+EMG_FP64, EMG_MIXED, EMG_EXACT = 0, 1, 2
 EMG_OUT_LINCOMB, EMG_OUT_K, EMG_OUT_M = 0, 1, 2
 
 # every symbol include/emgpu.h declares

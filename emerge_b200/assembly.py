@@ -17,8 +17,11 @@ complex128 data. ``np.asarray(Evec)`` materialises the reference COO layout.
 Differences from the reference, on purpose:
 * a zero-volume, non-finite or index-invalid tet raises ``EmgMeshError``
   (the reference silently produces inf/NaN entries);
-* ``precision="mixed"`` selects the FP32-contraction form (relative error
-  <= 1e-6 against FP64); the default is the plain FP64 form.
+* ``precision="fp64"`` (default) reproduces the reference's own FP64
+  arithmetic; ``"mixed"`` runs the quadrature products in FP32 (relative
+  error <= 1e-6 against FP64); ``"exact"`` evaluates the element integrals
+  in closed form, free of the reference's absolute-coordinate cancellation
+  (it then differs from the reference by the reference's rounding error).
 """
 from __future__ import annotations
 
@@ -48,9 +51,10 @@ def _to_dev(a: np.ndarray, dtype: torch.dtype, dev: torch.device) -> torch.Tenso
 
 
 def _prec(precision: str) -> int:
-    p = {"fp64": L.EMG_FP64, "plain": L.EMG_FP64, "mixed": L.EMG_MIXED}.get(str(precision).lower())
+    p = {"fp64": L.EMG_FP64, "plain": L.EMG_FP64, "mixed": L.EMG_MIXED,
+         "exact": L.EMG_EXACT}.get(str(precision).lower())
     if p is None:
-        raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        raise ValueError(f"precision must be 'fp64', 'mixed' or 'exact', got {precision!r}")
     return p
 
 

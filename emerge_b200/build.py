@@ -32,9 +32,9 @@ def _nvcc() -> str:
 
 def _units():
     units = [("api", "api.cu", []), ("plan", "plan.cu", []), ("gather", "gather.cu", [])]
-    for kind in (0, 1, 2):
-        for prec in (0, 1):
-            units.append((f"element_{kind}_{prec}", "element_inst.cu", [f"-DEMG_KIND={kind}", f"-DEMG_PREC={prec}"]))
+    for form in (0, 1, 2):
+        for kind in (0, 1, 2):
+            units.append((f"element_{form}_{kind}", "element_inst.cu", [f"-DEMG_FORM={form}", f"-DEMG_KIND={kind}"]))
     return units
 
 

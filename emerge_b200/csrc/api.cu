@@ -21,18 +21,19 @@ namespace {
 __global__ void k_probe() {}
 
 int launch_element(const ElemArgs &a, int kind, int precision, int out, cudaStream_t s) {
-  if (precision == EMG_FP64) {
-    if (kind == EMG_MAT_ISO) return launch_element_0_0(a, out, s);
-    if (kind == EMG_MAT_DIAG) return launch_element_1_0(a, out, s);
-    if (kind == EMG_MAT_FULL) return launch_element_2_0(a, out, s);
-  } else if (precision == EMG_MIXED) {
-    if (kind == EMG_MAT_ISO) return launch_element_0_1(a, out, s);
-    if (kind == EMG_MAT_DIAG) return launch_element_1_1(a, out, s);
-    if (kind == EMG_MAT_FULL) return launch_element_2_1(a, out, s);
-  } else {
-    return fail(EMG_EINVAL, "bad precision %d", precision);
+  if (kind < EMG_MAT_ISO || kind > EMG_MAT_FULL) return fail(EMG_EINVAL, "bad material kind %d", kind);
+  switch (precision * 3 + kind) {
+    case 0: return launch_element_0_0(a, out, s);
+    case 1: return launch_element_0_1(a, out, s);
+    case 2: return launch_element_0_2(a, out, s);
+    case 3: return launch_element_1_0(a, out, s);
+    case 4: return launch_element_1_1(a, out, s);
+    case 5: return launch_element_1_2(a, out, s);
+    case 6: return launch_element_2_0(a, out, s);
+    case 7: return launch_element_2_1(a, out, s);
+    case 8: return launch_element_2_2(a, out, s);
   }
-  return fail(EMG_EINVAL, "bad material kind %d", kind);
+  return fail(EMG_EINVAL, "bad precision %d", precision);
 }
 }  // namespace
 
@@ -131,7 +132,8 @@ int emg_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, c
 
 size_t emg_assemble_workspace_size(int64_t n_assy, int precision) {
   if (n_assy < 0) return 0;
-  return (size_t)n_assy * 400 * (precision == EMG_MIXED ? 8 : 16);
+  if (precision < EMG_FP64 || precision > EMG_EXACT) return 0;
+  return (size_t)n_assy * 400 * (values_fp32(precision) ? 8 : 16);
 }
 
 int emg_assemble(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const double *d_nodes,

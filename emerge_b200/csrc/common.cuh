@@ -70,14 +70,21 @@ struct ElemArgs {
   int64_t *st;
 };
 
-// element kernel launchers, one translation unit per (kind, precision)
-#define EMG_DECLARE_ELEM(K, P) int launch_element_##K##_##P(const ElemArgs &a, int out, cudaStream_t s);
+// element kernel launchers, one translation unit per (form, material kind);
+// form 0 = reference-faithful FP64, 1 = mixed, 2 = exact closed form
+#define EMG_DECLARE_ELEM(F, K) int launch_element_##F##_##K(const ElemArgs &a, int out, cudaStream_t s);
 EMG_DECLARE_ELEM(0, 0)
 EMG_DECLARE_ELEM(0, 1)
+EMG_DECLARE_ELEM(0, 2)
 EMG_DECLARE_ELEM(1, 0)
 EMG_DECLARE_ELEM(1, 1)
+EMG_DECLARE_ELEM(1, 2)
 EMG_DECLARE_ELEM(2, 0)
 EMG_DECLARE_ELEM(2, 1)
+EMG_DECLARE_ELEM(2, 2)
+
+// element values are complex64 for the mixed form, complex128 otherwise
+inline bool values_fp32(int precision) { return precision == EMG_MIXED; }
 
 // plan.cu
 size_t plan_workspace_bytes(const emg_plan *p);

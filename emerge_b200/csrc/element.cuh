@@ -1,23 +1,41 @@
-// element.cuh -- per-tet Nedelec-2 element kernel (closed-form K_e, M_e).
+// element.cuh -- per-tet Nedelec-2 element kernel.
 //
 // Replaces _matrix_builder + ned2_tet_stiff_mass + tet_coefficients +
 // local_mapping + matinv (physics/microwave/assembly/curlcurl.py:127-214,
-// 285-456; mth/optimized.py:262-357). Thread per assembled tet:
-//  * FP64: vertex ranks (the reference orients every edge/face by ascending
-//    global node id), barycentric gradients, |det| (V) and sign(det) in the
-//    tet's own vertex order (the reference's L = cofactor/|det| convention),
-//    material tensors and mu^-1 (the reference's matinv);
-//  * the element integrals are exact closed forms (KEAST4 integrates every
-//    integrand of this element space exactly), evaluated as straight-line
-//    multiply-adds on the per-tet tensors G = V (eps g_m).g_n and
-//    H = V (mu^-1 X_P).X_Q, in FP64 (EMG_FP64) or FP32 (EMG_MIXED);
-//  * one 20-value row of the block at a time goes to shared memory and the
-//    warp writes its 32 rows as contiguous runs of the [tet][a][b] layout.
+// 285-456; mth/optimized.py:262-357). Thread per assembled tet, three forms:
+//
+//  FORM_REF64 (EMG_FP64, plain) reproduces the reference's arithmetic: its
+//    barycentric coefficients from absolute-coordinate cofactors, its KEAST4
+//    points and its values L~ of the four barycentric functions at them, all
+//    in FP64 without fused multiply-adds in the reference's operation order.
+//    The 11-point sums are then evaluated exactly as the per-tet quadrature
+//    moments mu[alpha] = sum_q w_q L~_q^alpha (degree <= 4) contracted with
+//    the tensors G = V (eps grad L~_m).grad L~_n and H = V (mu^-1 X_P).X_Q
+//    through generated tables (nedelec_moment_tables.cuh).
+//  FORM_REF32 (EMG_MIXED): the same FP64 geometry and L~; the quadrature
+//    products (moments), tensors and their contraction in FP32 with FP32
+//    accumulation; element values complex64.
+//  FORM_EXACT (EMG_EXACT): exact closed-form integrals (nedelec_tables.cuh)
+//    on accurate edge-vector geometry, free of the reference's cancellation.
+//
+// Every form writes the reference's COO layout value[ia*400 + 20*a + b]: one
+// 20-value row of the block at a time is staged in shared memory and the warp
+// writes its 32 rows as contiguous 320-byte (160-byte) runs.
 #pragma once
 #include "common.cuh"
 
 namespace emg {
 namespace {
+
+enum { FORM_REF64 = 0, FORM_REF32 = 1, FORM_EXACT = 2 };
+template <int FORM>
+struct FormReal {
+  using T = double;
+};
+template <>
+struct FormReal<FORM_REF32> {
+  using T = float;
+};
 
 struct C64 {
   double re, im;
@@ -73,11 +91,32 @@ __device__ void matinv3(const C64 M[9], C64 out[9]) {
   for (int i = 0; i < 9; ++i) out[i] = cdiv(a[i], det);
 }
 
+
+// KEAST4 11-point rule exactly as the reference prints it (curlcurl.py:277-283):
+// row 0 weights, rows 1-4 barycentric coordinates of the points.
+__constant__ double kDP[5][11] = {
+    {-0.07893333333333329982, 0.04573333333333329948, 0.04573333333333329948, 0.04573333333333329948,
+     0.04573333333333329948, 0.14933333333333329018, 0.14933333333333329018, 0.14933333333333329018,
+     0.14933333333333329018, 0.14933333333333329018, 0.14933333333333329018},
+    {0.25000000000000000000, 0.78571428571428569843, 0.07142857142857139685, 0.07142857142857139685,
+     0.07142857142857139685, 0.10059642383320080428, 0.39940357616679922348, 0.39940357616679922348,
+     0.39940357616679922348, 0.10059642383320080428, 0.10059642383320080428},
+    {0.25000000000000000000, 0.07142857142857139685, 0.07142857142857139685, 0.07142857142857139685,
+     0.78571428571428569843, 0.39940357616679922348, 0.10059642383320080428, 0.39940357616679922348,
+     0.10059642383320080428, 0.39940357616679922348, 0.10059642383320080428},
+    {0.25000000000000000000, 0.07142857142857139685, 0.07142857142857139685, 0.78571428571428569843,
+     0.07142857142857139685, 0.39940357616679922348, 0.39940357616679922348, 0.10059642383320080428,
+     0.10059642383320080428, 0.10059642383320080428, 0.39940357616679922348},
+    {0.25000000000000000000, 0.07142857142857150787, 0.78571428571428580945, 0.07142857142857150787,
+     0.07142857142857150787, 0.10059642383320077652, 0.10059642383320077652, 0.10059642383320074877,
+     0.39940357616679922348, 0.39940357616679922348, 0.39940357616679922348},
+};
+
 // Per-tet geometry in the canonical (vertex-rank) frame.
 struct Geo {
-  double g[4][3];  // grad(lambda_r), r = rank of the vertex's global id
-  double V;        // |det| / 6
-  double sig;      // sign(det) in the tet's own vertex order
+  double g[4][3];  // gradients by vertex rank: reference forms grad L~, exact form grad lambda
+  double V;        // |det| / 6 (reference determinant in the reference forms)
+  double sig;      // sign(det) in the tet's own vertex order (exact form only)
   uint64_t inv;    // nibble c (0..9 canonical entity) -> reference entity slot (0..9)
 };
 
@@ -87,9 +126,84 @@ __device__ __forceinline__ int canon_edge(int a, int b) {
   return r1 == 0 ? r2 - 1 : (r1 == 1 ? r2 + 1 : 5);
 }
 
-// returns false for a degenerate tet (repeated vertex, zero/non-finite det)
-__device__ __forceinline__ bool tet_geometry(const double X[3][4], const int64_t v[4], Geo &G) {
-  int rank[4];
+// Barycentric coefficients exactly as the reference forms them
+// (tet_coefficients, curlcurl.py:127-214): 24-term determinant and signed
+// cofactors in ABSOLUTE coordinates, evaluated left to right without fused
+// multiply-adds, V = |det| / 6, coefficient = cofactor / (6 V). These
+// expressions cancel heavily (terms ~|x|^3 against det ~h^3), so the
+// reference's element matrices carry that rounding; reproducing the same
+// operation order keeps the GPU values within ulps of the reference's
+// instead of differing by the cancellation error.
+#define EMG_M2(a, b) __dmul_rn((a), (b))
+#define EMG_M3(a, b, c) __dmul_rn(__dmul_rn((a), (b)), (c))
+#define EMG_A(a, b) __dadd_rn((a), (b))
+#define EMG_S(a, b) __dsub_rn((a), (b))
+
+__device__ __forceinline__ void ref_coefficients(const double X[3][4], double ca[4], double cb[4], double cc[4],
+                                                 double cd[4], double &det) {
+  const double x1 = X[0][0], x2 = X[0][1], x3 = X[0][2], x4 = X[0][3];
+  const double y1 = X[1][0], y2 = X[1][1], y3 = X[1][2], y4 = X[1][3];
+  const double z1 = X[2][0], z2 = X[2][1], z3 = X[2][2], z4 = X[2][3];
+  double d = EMG_M3(-x1, y2, z3);
+  d = EMG_A(d, EMG_M3(x1, y2, z4));
+  d = EMG_A(d, EMG_M3(x1, y3, z2));
+  d = EMG_S(d, EMG_M3(x1, y3, z4));
+  d = EMG_S(d, EMG_M3(x1, y4, z2));
+  d = EMG_A(d, EMG_M3(x1, y4, z3));
+  d = EMG_A(d, EMG_M3(x2, y1, z3));
+  d = EMG_S(d, EMG_M3(x2, y1, z4));
+  d = EMG_S(d, EMG_M3(x2, y3, z1));
+  d = EMG_A(d, EMG_M3(x2, y3, z4));
+  d = EMG_A(d, EMG_M3(x2, y4, z1));
+  d = EMG_S(d, EMG_M3(x2, y4, z3));
+  d = EMG_S(d, EMG_M3(x3, y1, z2));
+  d = EMG_A(d, EMG_M3(x3, y1, z4));
+  d = EMG_A(d, EMG_M3(x3, y2, z1));
+  d = EMG_S(d, EMG_M3(x3, y2, z4));
+  d = EMG_S(d, EMG_M3(x3, y4, z1));
+  d = EMG_A(d, EMG_M3(x3, y4, z2));
+  d = EMG_A(d, EMG_M3(x4, y1, z2));
+  d = EMG_S(d, EMG_M3(x4, y1, z3));
+  d = EMG_S(d, EMG_M3(x4, y2, z1));
+  d = EMG_A(d, EMG_M3(x4, y2, z3));
+  d = EMG_A(d, EMG_M3(x4, y3, z1));
+  d = EMG_S(d, EMG_M3(x4, y3, z2));
+  det = d;
+  // six-term cofactor sums (the reference's bbs, ccs, dds)
+#define EMG_C6(s1, a1, b1, s2, a2, b2, s3, a3, b3, s4, a4, b4, s5, a5, b5, s6, a6, b6)                   \
+  EMG_##s6(EMG_##s5(EMG_##s4(EMG_##s3(EMG_##s2(EMG_M2(s1 a1, b1), EMG_M2(a2, b2)), EMG_M2(a3, b3)),       \
+                             EMG_M2(a4, b4)),                                                             \
+                    EMG_M2(a5, b5)),                                                                      \
+           EMG_M2(a6, b6))
+  cb[0] = EMG_C6(-, y2, z3, A, y2, z4, A, y3, z2, S, y3, z4, S, y4, z2, A, y4, z3);
+  cb[1] = EMG_C6(+, y1, z3, S, y1, z4, S, y3, z1, A, y3, z4, A, y4, z1, S, y4, z3);
+  cb[2] = EMG_C6(-, y1, z2, A, y1, z4, A, y2, z1, S, y2, z4, S, y4, z1, A, y4, z2);
+  cb[3] = EMG_C6(+, y1, z2, S, y1, z3, S, y2, z1, A, y2, z3, A, y3, z1, S, y3, z2);
+  cc[0] = EMG_C6(+, x2, z3, S, x2, z4, S, x3, z2, A, x3, z4, A, x4, z2, S, x4, z3);
+  cc[1] = EMG_C6(-, x1, z3, A, x1, z4, A, x3, z1, S, x3, z4, S, x4, z1, A, x4, z3);
+  cc[2] = EMG_C6(+, x1, z2, S, x1, z4, S, x2, z1, A, x2, z4, A, x4, z1, S, x4, z2);
+  cc[3] = EMG_C6(-, x1, z2, A, x1, z3, A, x2, z1, S, x2, z3, S, x3, z1, A, x3, z2);
+  cd[0] = EMG_C6(-, x2, y3, A, x2, y4, A, x3, y2, S, x3, y4, S, x4, y2, A, x4, y3);
+  cd[1] = EMG_C6(+, x1, y3, S, x1, y4, S, x3, y1, A, x3, y4, A, x4, y1, S, x4, y3);
+  cd[2] = EMG_C6(-, x1, y2, A, x1, y4, A, x2, y1, S, x2, y4, S, x4, y1, A, x4, y2);
+  cd[3] = EMG_C6(+, x1, y2, S, x1, y3, S, x2, y1, A, x2, y3, A, x3, y1, S, x3, y2);
+#undef EMG_C6
+  // six-term triple-product sums (the reference's aas)
+#define EMG_T6(s1, a1, b1, c1, s2, a2, b2, c2, s3, a3, b3, c3, s4, a4, b4, c4, s5, a5, b5, c5, s6, a6, b6, c6)   \
+  EMG_##s6(EMG_##s5(EMG_##s4(EMG_##s3(EMG_##s2(EMG_M3(s1 a1, b1, c1), EMG_M3(a2, b2, c2)), EMG_M3(a3, b3, c3)),     \
+                             EMG_M3(a4, b4, c4)),                                                                \
+                    EMG_M3(a5, b5, c5)),                                                                         \
+           EMG_M3(a6, b6, c6))
+  ca[0] = EMG_T6(+, x2, y3, z4, S, x2, y4, z3, S, x3, y2, z4, A, x3, y4, z2, A, x4, y2, z3, S, x4, y3, z2);
+  ca[1] = EMG_T6(-, x1, y3, z4, A, x1, y4, z3, A, x3, y1, z4, S, x3, y4, z1, S, x4, y1, z3, A, x4, y3, z1);
+  ca[2] = EMG_T6(+, x1, y2, z4, S, x1, y4, z2, S, x2, y1, z4, A, x2, y4, z1, A, x4, y1, z2, S, x4, y2, z1);
+  ca[3] = EMG_T6(-, x1, y2, z3, A, x1, y3, z2, A, x2, y1, z3, S, x2, y3, z1, S, x3, y1, z2, A, x3, y2, z1);
+#undef EMG_T6
+}
+
+
+// vertex ranks by global id, and the canonical -> reference entity map
+__device__ __forceinline__ bool ranks_and_map(const int64_t v[4], int rank[4], uint64_t &inv) {
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     int r = 0;
@@ -97,8 +211,133 @@ __device__ __forceinline__ bool tet_geometry(const double X[3][4], const int64_t
     for (int p = 0; p < 4; ++p) r += (v[p] < v[q]) ? 1 : 0;
     rank[q] = r;
   }
-  bool distinct = (v[0] != v[1]) && (v[0] != v[2]) && (v[0] != v[3]) && (v[1] != v[2]) && (v[1] != v[3]) &&
-                  (v[2] != v[3]);
+  const bool distinct = (v[0] != v[1]) && (v[0] != v[2]) && (v[0] != v[3]) && (v[1] != v[2]) && (v[1] != v[3]) &&
+                        (v[2] != v[3]);
+  // reference edge slots (local vertex pairs) and the vertex missing from each face slot
+  const int eu[6] = {0, 0, 0, 1, 3, 2}, ev[6] = {1, 2, 3, 2, 1, 3};
+  const int fmiss[4] = {3, 1, 2, 0};
+  uint64_t m = 0;
+  if (distinct) {
+#pragma unroll
+    for (int s = 0; s < 6; ++s) m |= (uint64_t)s << (4 * canon_edge(rank[eu[s]], rank[ev[s]]));
+#pragma unroll
+    for (int f = 0; f < 4; ++f) m |= (uint64_t)(6 + f) << (4 * (6 + 3 - rank[fmiss[f]]));
+  }
+  inv = m;
+  return distinct;
+}
+
+template <typename T>
+__device__ __forceinline__ void scatter_rank(const T in[4], const int rank[4], T out[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      if (rank[q] == r) out[r] = in[q];
+}
+
+}  // namespace
+
+// the generated tables call emg_mac unqualified: include them inside emg
+template <typename R>
+struct CR {
+  R re, im;
+};
+// Every multiply-add of the generated tables goes through rounding
+// intrinsics, which the compiler neither re-associates nor re-contracts: the
+// (x, y) and (y, x) entries, computed in different rows, are then bitwise
+// equal, so the element blocks and A stay exactly symmetric.
+__device__ __forceinline__ void emg_mac(double &acc, double a, double b) { acc = __fma_rn(a, b, acc); }
+__device__ __forceinline__ void emg_mac(float &acc, double c, float v) { acc = __fmaf_rn((float)c, v, acc); }
+__device__ __forceinline__ void emg_mac(float &acc, float a, float b) { acc = __fmaf_rn(a, b, acc); }
+__device__ __forceinline__ void emg_mac(CR<double> &acc, double c, const CR<double> &v) {
+  acc.re = __fma_rn(c, v.re, acc.re);
+  acc.im = __fma_rn(c, v.im, acc.im);
+}
+__device__ __forceinline__ void emg_mac(CR<float> &acc, double c, const CR<float> &v) {
+  acc.re = __fmaf_rn((float)c, v.re, acc.re);
+  acc.im = __fmaf_rn((float)c, v.im, acc.im);
+}
+__device__ __forceinline__ void emg_mac(CR<double> &acc, const CR<double> &t, double w) {
+  acc.re = __fma_rn(t.re, w, acc.re);
+  acc.im = __fma_rn(t.im, w, acc.im);
+}
+__device__ __forceinline__ void emg_mac(CR<float> &acc, const CR<float> &t, float w) {
+  acc.re = __fmaf_rn(t.re, w, acc.re);
+  acc.im = __fmaf_rn(t.im, w, acc.im);
+}
+// inner moment sums of the generated tables: c0*mu0, then fma(c, mu, t)
+__device__ __forceinline__ double emg_mul(double c, double m) { return __dmul_rn(c, m); }
+__device__ __forceinline__ float emg_mul(double c, float m) { return __fmul_rn((float)c, m); }
+__device__ __forceinline__ double emg_fma(double t, double c, double m) { return __fma_rn(c, m, t); }
+__device__ __forceinline__ float emg_fma(float t, double c, float m) { return __fmaf_rn((float)c, m, t); }
+#include "nedelec_moment_tables.cuh"
+#include "nedelec_tables.cuh"
+
+namespace {
+
+constexpr int NMOM = emg_mtables::kNumMoments;
+
+// Reference forms: coefficients, quadrature points and L~ exactly as the
+// reference computes them, then the quadrature moments. Returns false for a
+// degenerate tet.
+template <typename R>
+__device__ __forceinline__ bool ref_geometry(const double X[3][4], const int64_t v[4], Geo &G, R mu[NMOM]) {
+  int rank[4];
+  uint64_t inv;
+  const bool distinct = ranks_and_map(v, rank, inv);
+  double ca[4], cb[4], cc[4], cd[4], det;
+  ref_coefficients(X, ca, cb, cc, cd, det);
+  if (!distinct || !(det != 0.0) || !isfinite(det)) return false;
+  const double V = fabs(det) / 6.0;
+  const double six_v = __dmul_rn(6.0, V);
+  double a[4], b[4], c[4], d[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    a[q] = ca[q] / six_v;
+    b[q] = cb[q] / six_v;
+    c[q] = cc[q] / six_v;
+    d[q] = cd[q] / six_v;
+  }
+  double br[4], cr[4], dr[4];
+  scatter_rank(b, rank, br);
+  scatter_rank(c, rank, cr);
+  scatter_rank(d, rank, dr);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    G.g[r][0] = br[r];
+    G.g[r][1] = cr[r];
+    G.g[r][2] = dr[r];
+  }
+  G.V = V;
+  G.sig = 1.0;
+  G.inv = inv;
+#pragma unroll
+  for (int i = 0; i < NMOM; ++i) mu[i] = (R)0;
+#pragma unroll
+  for (int q = 0; q < 11; ++q) {
+    const double p1 = kDP[1][q], p2 = kDP[2][q], p3 = kDP[3][q], p4 = kDP[4][q];
+    double xq[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      xq[k] = EMG_A(EMG_A(EMG_A(EMG_M2(X[k][0], p1), EMG_M2(X[k][1], p2)), EMG_M2(X[k][2], p3)), EMG_M2(X[k][3], p4));
+    double L[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+      L[m] = EMG_A(EMG_A(EMG_A(a[m], EMG_M2(b[m], xq[0])), EMG_M2(c[m], xq[1])), EMG_M2(d[m], xq[2]));
+    double Lr[4];
+    scatter_rank(L, rank, Lr);
+    R Lq[4] = {(R)Lr[0], (R)Lr[1], (R)Lr[2], (R)Lr[3]};
+    emg_mtables::emg_moments<R>(Lq, (R)kDP[0][q], mu);
+  }
+  return true;
+}
+
+// Exact form: accurate gradients from edge vectors (relative to vertex 0).
+__device__ __forceinline__ bool exact_geometry(const double X[3][4], const int64_t v[4], Geo &G) {
+  int rank[4];
+  uint64_t inv;
+  const bool distinct = ranks_and_map(v, rank, inv);
   double e1[3], e2[3], e3[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -111,34 +350,26 @@ __device__ __forceinline__ bool tet_geometry(const double X[3][4], const int64_t
   double c12[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
   double det = e1[0] * c23[0] + e1[1] * c23[1] + e1[2] * c23[2];
   if (!distinct || !(det != 0.0) || !isfinite(det)) return false;
-  double id = 1.0 / det;
-  double gl[4][3];
+  const double id = 1.0 / det;
+  double gx[4], gy[4], gz[4];
+  gx[1] = c23[0] * id, gy[1] = c23[1] * id, gz[1] = c23[2] * id;
+  gx[2] = c31[0] * id, gy[2] = c31[1] * id, gz[2] = c31[2] * id;
+  gx[3] = c12[0] * id, gy[3] = c12[1] * id, gz[3] = c12[2] * id;
+  gx[0] = -(gx[1] + gx[2] + gx[3]);
+  gy[0] = -(gy[1] + gy[2] + gy[3]);
+  gz[0] = -(gz[1] + gz[2] + gz[3]);
+  double rx[4], ry[4], rz[4];
+  scatter_rank(gx, rank, rx);
+  scatter_rank(gy, rank, ry);
+  scatter_rank(gz, rank, rz);
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    gl[1][d] = c23[d] * id;
-    gl[2][d] = c31[d] * id;
-    gl[3][d] = c12[d] * id;
-    gl[0][d] = -(gl[1][d] + gl[2][d] + gl[3][d]);
+  for (int r = 0; r < 4; ++r) {
+    G.g[r][0] = rx[r];
+    G.g[r][1] = ry[r];
+    G.g[r][2] = rz[r];
   }
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      // scatter by rank without dynamic register indexing
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (rank[q] == r) G.g[r][d] = gl[q][d];
-    }
   G.V = fabs(det) / 6.0;
   G.sig = det > 0.0 ? 1.0 : -1.0;
-  // reference edge slots (local vertex pairs) and the vertex missing from each face slot
-  const int eu[6] = {0, 0, 0, 1, 3, 2}, ev[6] = {1, 2, 3, 2, 1, 3};
-  const int fmiss[4] = {3, 1, 2, 0};
-  uint64_t inv = 0;
-#pragma unroll
-  for (int s = 0; s < 6; ++s) inv |= (uint64_t)s << (4 * canon_edge(rank[eu[s]], rank[ev[s]]));
-#pragma unroll
-  for (int f = 0; f < 4; ++f) inv |= (uint64_t)(6 + f) << (4 * (6 + 3 - rank[fmiss[f]]));
   G.inv = inv;
   return true;
 }
@@ -150,46 +381,15 @@ __device__ __forceinline__ int ref_dof(uint64_t inv, int y) {
   return y < 6 ? s : (y < 12 ? 6 + s : (y < 16 ? 12 + (s - 6) : 16 + (s - 6)));
 }
 
-template <typename R>
-struct CR {
-  R re, im;
-};
-
-// multiply-add used by the generated tables: acc += c * v
-__device__ __forceinline__ void emg_mac(double &acc, double c, double v) { acc = fma(c, v, acc); }
-__device__ __forceinline__ void emg_mac(float &acc, double c, float v) { acc = fmaf((float)c, v, acc); }
-__device__ __forceinline__ void emg_mac(CR<double> &acc, double c, const CR<double> &v) {
-  acc.re = fma(c, v.re, acc.re);
-  acc.im = fma(c, v.im, acc.im);
-}
-__device__ __forceinline__ void emg_mac(CR<float> &acc, double c, const CR<float> &v) {
-  acc.re = fmaf((float)c, v.re, acc.re);
-  acc.im = fmaf((float)c, v.im, acc.im);
-}
-
-}  // namespace
-
-// the generated tables call emg_mac unqualified: include them inside emg
-#include "nedelec_tables.cuh"
-
-namespace {
-
-// Contractions: real symmetric (ISO) and complex (DIAG symmetric, FULL general).
-// Tensor T_G[m][n] = (eps g_m).g_n * V, T_H[P][Q] = (mu^-1 X_P).X_Q * V.
+// Per-tet tensors, V folded in: G[m][n] = V (eps g_m).g_n, H[P][Q] = V (mu^-1 X_P).X_Q.
+// ISO: real (material scalars applied per entry); DIAG symmetric / FULL general: complex.
 template <int KIND, typename R>
-struct Tensors;
-
+struct Tensors {
+  CR<R> G[4][4], H[6][6];
+};
 template <typename R>
 struct Tensors<EMG_MAT_ISO, R> {
-  R G[4][4], H[6][6];  // real, symmetric, V folded in; material scalars applied per entry
-};
-template <typename R>
-struct Tensors<EMG_MAT_DIAG, R> {
-  CR<R> G[4][4], H[6][6];
-};
-template <typename R>
-struct Tensors<EMG_MAT_FULL, R> {
-  CR<R> G[4][4], H[6][6];
+  R G[4][4], H[6][6];
 };
 
 __device__ __forceinline__ void cross3(const double a[3], const double b[3], double o[3]) {
@@ -220,15 +420,13 @@ __device__ __forceinline__ void build_iso(const Geo &Gm, Tensors<EMG_MAT_ISO, R>
     }
 }
 
-// general complex tensors: eps, minv are 3x3 row-major complex
+// complex tensors: eps, minv are 3x3 row-major complex; (A u).w = sum_r w_r sum_c A[r][c] u_c
 template <int KIND, typename R>
-__device__ __forceinline__ void build_cplx(const Geo &Gm, const C64 eps[9], const C64 minv[9],
-                                           Tensors<KIND, R> &T) {
+__device__ __forceinline__ void build_cplx(const Geo &Gm, const C64 eps[9], const C64 minv[9], Tensors<KIND, R> &T) {
   double X[6][3];
   const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
 #pragma unroll
   for (int p = 0; p < 6; ++p) cross3(Gm.g[pa[p]], Gm.g[pb[p]], X[p]);
-  // (A u).w = sum_r w_r sum_c A[r][c] u_c
 #pragma unroll
   for (int m = 0; m < 4; ++m)
 #pragma unroll
@@ -271,30 +469,42 @@ __device__ __forceinline__ void build_cplx(const Geo &Gm, const C64 eps[9], cons
     }
 }
 
-// entry (first=f, second=s) of K and M in the canonical frame
-template <int f, int s, typename R>
-__device__ __forceinline__ void entry_iso(const Tensors<EMG_MAT_ISO, R> &T, R sig, R &k, R &m) {
-  R ak = 0, am = 0;
-  emg_tables::Pair<f, s>::stiff(ak, T.H);
-  emg_tables::Pair<f, s>::mass(am, T.G);
-  if (emg_tables::odd(f) != emg_tables::odd(s)) {
-    ak *= sig;
-    am *= sig;
-  }
-  k = ak;
-  m = am;
-}
+template <int KIND, typename R>
+struct EntryT {
+  using T = CR<R>;
+};
+template <typename R>
+struct EntryT<EMG_MAT_ISO, R> {
+  using T = R;
+};
 
-template <int f, int s, int KIND, typename R>
-__device__ __forceinline__ void entry_cplx(const Tensors<KIND, R> &T, R sig, CR<R> &k, CR<R> &m) {
-  CR<R> ak{0, 0}, am{0, 0};
-  emg_tables::Pair<f, s>::stiff(ak, T.H);
-  emg_tables::Pair<f, s>::mass(am, T.G);
-  if (emg_tables::odd(f) != emg_tables::odd(s)) {
-    ak.re *= sig;
-    ak.im *= sig;
-    am.re *= sig;
-    am.im *= sig;
+template <typename A>
+__device__ __forceinline__ void scale_sign(A &x, double s);
+template <>
+__device__ __forceinline__ void scale_sign(double &x, double s) { x *= s; }
+template <>
+__device__ __forceinline__ void scale_sign(float &x, double s) { x *= (float)s; }
+template <>
+__device__ __forceinline__ void scale_sign(CR<double> &x, double s) { x.re *= s, x.im *= s; }
+template <>
+__device__ __forceinline__ void scale_sign(CR<float> &x, double s) { x.re *= (float)s, x.im *= (float)s; }
+
+// entry (first=f, second=s) of K and M in the canonical frame
+template <int f, int s, int FORM, int KIND, typename R>
+__device__ __forceinline__ void entry(const Tensors<KIND, R> &T, const R *mu, double sig,
+                                      typename EntryT<KIND, R>::T &k, typename EntryT<KIND, R>::T &m) {
+  using E = typename EntryT<KIND, R>::T;
+  E ak{}, am{};
+  if constexpr (FORM == FORM_EXACT) {
+    emg_tables::Pair<f, s>::stiff(ak, T.H);
+    emg_tables::Pair<f, s>::mass(am, T.G);
+    if (emg_tables::odd(f) != emg_tables::odd(s)) {
+      scale_sign(ak, sig);
+      scale_sign(am, sig);
+    }
+  } else {
+    emg_mtables::MPair<f, s>::stiff(ak, T.H, mu);
+    emg_mtables::MPair<f, s>::mass(am, T.G, mu);
   }
   k = ak;
   m = am;
@@ -314,57 +524,56 @@ struct StoreT<float> {
 constexpr int ELEM_THREADS = 128;
 constexpr int ELEM_WARPS = ELEM_THREADS / 32;
 
+__device__ __forceinline__ double cfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float cfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double cmul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float cmul_rn(float a, float b) { return __fmul_rn(a, b); }
 
-// per-tet complex scale factors for the ISO kind: value = cK*K0 + cM*M0
-template <int KIND, int OUT, typename R>
-struct RowCtx;
-
-template <int x, int y, int KIND, int OUT, typename R>
-__device__ __forceinline__ void compute_store(const Tensors<KIND, R> &T, R sig, const CR<R> &cK, const CR<R> &cM,
-                                              uint64_t inv, int rx, typename StoreT<R>::T *row) {
+template <int x, int y, int FORM, int KIND, typename R>
+__device__ __forceinline__ void compute_store(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                              const CR<R> &cM, uint64_t inv, int rx, typename StoreT<R>::T *row) {
   using ST = typename StoreT<R>::T;
   const int b = ref_dof(inv, y);
   ST v;
   if constexpr (KIND == EMG_MAT_ISO) {
     R k0, m0;
-    entry_iso<(x < y ? x : y), (x < y ? y : x)>(T, sig, k0, m0);
-    v.x = cK.re * k0 + cM.re * m0;
-    v.y = cK.im * k0 + cM.im * m0;
+    entry<(x < y ? x : y), (x < y ? y : x), FORM, KIND, R>(T, mu, sig, k0, m0);
+    v.x = cfma(cK.re, k0, cmul_rn(cM.re, m0));
+    v.y = cfma(cK.im, k0, cmul_rn(cM.im, m0));
   } else {
     CR<R> k, m;
     if constexpr (KIND == EMG_MAT_DIAG) {
-      entry_cplx<(x < y ? x : y), (x < y ? y : x), KIND>(T, sig, k, m);
+      entry<(x < y ? x : y), (x < y ? y : x), FORM, KIND, R>(T, mu, sig, k, m);
     } else {
       // first = the DoF with the lower reference index (curlcurl.py:358-376)
       if (rx <= b) {
-        entry_cplx<x, y, KIND>(T, sig, k, m);
+        entry<x, y, FORM, KIND, R>(T, mu, sig, k, m);
       } else {
-        entry_cplx<y, x, KIND>(T, sig, k, m);
+        entry<y, x, FORM, KIND, R>(T, mu, sig, k, m);
       }
     }
-    // value = cK*K + cM*M, cK/cM = (alpha, beta) or (1,0)/(0,1)
-    v.x = cK.re * k.re - cK.im * k.im + cM.re * m.re - cM.im * m.im;
-    v.y = cK.re * k.im + cK.im * k.re + cM.re * m.im + cM.im * m.re;
+    v.x = cfma(cK.re, k.re, cfma(-cK.im, k.im, cfma(cM.re, m.re, cmul_rn(-cM.im, m.im))));
+    v.y = cfma(cK.re, k.im, cfma(cK.im, k.re, cfma(cM.re, m.im, cmul_rn(cM.im, m.re))));
   }
   row[b] = v;
 }
 
-template <int x, int KIND, int OUT, typename R, int... Ys>
-__device__ __forceinline__ void compute_row(const Tensors<KIND, R> &T, R sig, const CR<R> &cK, const CR<R> &cM,
-                                            uint64_t inv, int rx, typename StoreT<R>::T *row,
+template <int x, int FORM, int KIND, typename R, int... Ys>
+__device__ __forceinline__ void compute_row(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                            const CR<R> &cM, uint64_t inv, int rx, typename StoreT<R>::T *row,
                                             std::integer_sequence<int, Ys...>) {
-  (compute_store<x, Ys, KIND, OUT, R>(T, sig, cK, cM, inv, rx, row), ...);
+  (compute_store<x, Ys, FORM, KIND, R>(T, mu, sig, cK, cM, inv, rx, row), ...);
 }
 
-template <int KIND, int OUT, typename R, int X>
-__device__ __forceinline__ void do_row(const Tensors<KIND, R> &T, R sig, const CR<R> &cK, const CR<R> &cM,
-                                       uint64_t inv, bool active, int ia, typename StoreT<R>::T *stage,
-                                       typename StoreT<R>::T *out) {
-  using ST = typename StoreT<R>::T;
+template <int FORM, int KIND, typename R, int X>
+__device__ __forceinline__ void do_row(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                       const CR<R> &cM, uint64_t inv, bool active, int ia,
+                                       typename StoreT<R>::T *stage, typename StoreT<R>::T *out) {
   const int lane = threadIdx.x & 31;
   const int rx = ref_dof(inv, X);
-  if (active) compute_row<X, KIND, OUT, R>(T, sig, cK, cM, inv, rx, stage + lane * 20,
-                                          std::make_integer_sequence<int, 20>{});
+  if (active)
+    compute_row<X, FORM, KIND, R>(T, mu, sig, cK, cM, inv, rx, stage + lane * 20,
+                                  std::make_integer_sequence<int, 20>{});
   __syncwarp();
   // cooperative, coalesced write of the warp's 32 rows (each 20 contiguous values)
 #pragma unroll 4
@@ -379,15 +588,17 @@ __device__ __forceinline__ void do_row(const Tensors<KIND, R> &T, R sig, const C
   __syncwarp();
 }
 
-template <int KIND, int OUT, typename R, int... Xs>
-__device__ __forceinline__ void all_rows(const Tensors<KIND, R> &T, R sig, const CR<R> &cK, const CR<R> &cM,
-                                         uint64_t inv, bool active, int ia, typename StoreT<R>::T *stage,
-                                         typename StoreT<R>::T *out, std::integer_sequence<int, Xs...>) {
-  (do_row<KIND, OUT, R, Xs>(T, sig, cK, cM, inv, active, ia, stage, out), ...);
+template <int FORM, int KIND, typename R, int... Xs>
+__device__ __forceinline__ void all_rows(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                         const CR<R> &cM, uint64_t inv, bool active, int ia,
+                                         typename StoreT<R>::T *stage, typename StoreT<R>::T *out,
+                                         std::integer_sequence<int, Xs...>) {
+  (do_row<FORM, KIND, R, Xs>(T, mu, sig, cK, cM, inv, active, ia, stage, out), ...);
 }
 
-template <int KIND, int OUT, typename R>
+template <int FORM, int KIND, int OUT>
 __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
+  using R = typename FormReal<FORM>::T;
   using ST = typename StoreT<R>::T;
   __shared__ ST stage_all[ELEM_WARPS][32 * 20];
   ST *stage = stage_all[threadIdx.x >> 5];
@@ -397,8 +608,9 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
   const int ia = (int)ia64;
   Geo G;
   Tensors<KIND, R> T;
+  R mu[FORM == FORM_EXACT ? 1 : NMOM];
   CR<R> cK{0, 0}, cM{0, 0};
-  R sig = 1;
+  double sig = 1.0;
   uint64_t inv = 0;
   if (active) {
     int64_t it = a.tetids ? (int64_t)a.tetids[ia] : ia64;
@@ -420,11 +632,17 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
       for (int q = 0; q < 4; ++q)
 #pragma unroll
         for (int d = 0; d < 3; ++d) X[d][q] = a.nodes[(int64_t)d * a.nN + v[q]];
-      if (!tet_geometry(X, v, G)) {
+      bool good;
+      if constexpr (FORM == FORM_EXACT) {
+        good = exact_geometry(X, v, G);
+      } else {
+        good = ref_geometry<R>(X, v, G, mu);
+      }
+      if (!good) {
         flag(a.st, EMG_ST_DEGENERATE, ia64);
         active = false;
       } else {
-        sig = (R)G.sig;
+        sig = G.sig;
         inv = G.inv;
         C64 alpha{a.ar, a.ai}, beta{a.br, a.bi};
         if (OUT == EMG_OUT_K) {
@@ -442,7 +660,7 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
           cM = {(R)m.re, (R)m.im};
           build_iso<R>(G, T);
         } else {
-          C64 eps[9], mu[9], minv[9];
+          C64 eps[9], mu3[9], minv[9];
 #pragma unroll
           for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -451,9 +669,9 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
               const bool need = (KIND == EMG_MAT_FULL) || r == c;
               const int64_t o = (KIND == EMG_MAT_FULL) ? (int64_t)(3 * r + c) * a.nT + it : (int64_t)r * a.nT + it;
               eps[3 * r + c] = need ? ld_c64(a.er, o) : C64{0.0, 0.0};
-              mu[3 * r + c] = (need && a.ur) ? ld_c64(a.ur, o) : C64{(r == c) ? 1.0 : 0.0, 0.0};
+              mu3[3 * r + c] = (need && a.ur) ? ld_c64(a.ur, o) : C64{(r == c) ? 1.0 : 0.0, 0.0};
             }
-          matinv3(mu, minv);
+          matinv3(mu3, minv);
           cK = {(R)alpha.re, (R)alpha.im};
           cM = {(R)beta.re, (R)beta.im};
           build_cplx<KIND, R>(G, eps, minv, T);
@@ -461,22 +679,22 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
       }
     }
   }
-  all_rows<KIND, OUT, R>(T, sig, cK, cM, inv, active, ia, stage, out, std::make_integer_sequence<int, 20>{});
+  all_rows<FORM, KIND, R>(T, mu, sig, cK, cM, inv, active, ia, stage, out, std::make_integer_sequence<int, 20>{});
 }
 
-template <int KIND, int OUT, typename R>
+template <int FORM, int KIND, int OUT>
 int launch_element_t(const ElemArgs &a, cudaStream_t s) {
   if (a.nA == 0) return EMG_OK;
-  k_element<KIND, OUT, R><<<grid_for(a.nA, ELEM_THREADS), ELEM_THREADS, 0, s>>>(a);
+  k_element<FORM, KIND, OUT><<<grid_for(a.nA, ELEM_THREADS), ELEM_THREADS, 0, s>>>(a);
   return launch_check("k_element");
 }
 
-template <int KIND, typename R>
+template <int FORM, int KIND>
 int launch_element_k(const ElemArgs &a, int out, cudaStream_t s) {
   switch (out) {
-    case EMG_OUT_LINCOMB: return launch_element_t<KIND, EMG_OUT_LINCOMB, R>(a, s);
-    case EMG_OUT_K: return launch_element_t<KIND, EMG_OUT_K, R>(a, s);
-    case EMG_OUT_M: return launch_element_t<KIND, EMG_OUT_M, R>(a, s);
+    case EMG_OUT_LINCOMB: return launch_element_t<FORM, KIND, EMG_OUT_LINCOMB>(a, s);
+    case EMG_OUT_K: return launch_element_t<FORM, KIND, EMG_OUT_K>(a, s);
+    case EMG_OUT_M: return launch_element_t<FORM, KIND, EMG_OUT_M>(a, s);
   }
   return fail(EMG_EINVAL, "bad output selector %d", out);
 }

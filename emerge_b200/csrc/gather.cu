@@ -137,12 +137,11 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
 #define EMG_GATHER(R, TWO)                                                                                         \
   k_gather<R, TWO><<<g, GATHER_WARPS * 32, 0, s>>>(ent_ptr, items, ent_cnt, p->n_ent, p->n_edges, p->n_tris,      \
                                                    d_indptr, d_v1, d_v2, ar, ai, br, bi, A, d_status)
-  if (precision == EMG_FP64) {
+  if (precision < EMG_FP64 || precision > EMG_EXACT) return fail(EMG_EINVAL, "bad precision %d", precision);
+  if (!values_fp32(precision)) {
     if (d_v2) EMG_GATHER(double, true); else EMG_GATHER(double, false);
-  } else if (precision == EMG_MIXED) {
-    if (d_v2) EMG_GATHER(float, true); else EMG_GATHER(float, false);
   } else {
-    return fail(EMG_EINVAL, "bad precision %d", precision);
+    if (d_v2) EMG_GATHER(float, true); else EMG_GATHER(float, false);
   }
 #undef EMG_GATHER
   return launch_check("k_gather");

@@ -157,6 +157,55 @@ def tables():
     return mass, stiff
 
 
+def monomials():
+    """All monomials of degree <= 4 in (L0, L1, L2, L3), by degree then
+    lexicographically descending exponents."""
+    out = []
+    for a in range(5):
+        for b in range(5 - a):
+            for c in range(5 - a - b):
+                for d in range(5 - a - b - c):
+                    out.append((a, b, c, d))
+    return sorted(out, key=lambda e: (sum(e), tuple(-x for x in e)))
+
+
+MONOS = monomials()
+MONO_INDEX = {e: i for i, e in enumerate(MONOS)}
+
+
+def moment_tables():
+    """Quadrature-moment form of the element integrals, for reproducing the
+    reference's rounding: with L~ the reference's barycentric values at the 11
+    KEAST4 points and mu[alpha] = sum_q w_q L~_q^alpha,
+
+        M[x,y] = V~ sum_(m,n) G~[m][n] * sum_(alpha,c) c * mu[alpha]
+        K[x,y] = V~ sum_(P,Q) H~[P][Q] * sum_(alpha,c) c * mu[alpha]
+
+    where the basis polynomials are written in L (no orientation signs:
+    L~ and grad L~ already carry them). Returns (mass, stiff): dict (x, y) ->
+    list of (a, b, [(monomial index, Fraction c), ...])."""
+    B = basis()
+    mass, stiff = {}, {}
+    for x in range(20):
+        vx, cx = B[x]
+        for y in range(20):
+            vy, cy = B[y]
+            mt, st = [], []
+            for m, pm in sorted(vx.items()):
+                for n, pn in sorted(vy.items()):
+                    prod = _pmul(pm, pn)
+                    if prod:
+                        mt.append((m, n, sorted((MONO_INDEX[e], c) for e, c in prod.items())))
+            for P, qp in sorted(cx.items()):
+                for Q, qq in sorted(cy.items()):
+                    prod = _pmul(qp, qq)
+                    if prod:
+                        st.append((P, Q, sorted((MONO_INDEX[e], c) for e, c in prod.items())))
+            mass[(x, y)] = mt
+            stiff[(x, y)] = st
+    return mass, stiff
+
+
 def _fmt(c: Fraction) -> str:
     return f"{float(c)!r}" if c.denominator != 1 else f"{c.numerator}.0"
 
@@ -196,5 +245,63 @@ def emit_header(path: str) -> None:
         f.write("\n".join(lines) + "\n")
 
 
+def emit_moment_header(path: str) -> None:
+    """Write the quadrature-moment tables: ``emg_moments(L, w, mu)`` adds one
+    point's weighted monomials w * L^alpha into mu[70], and ``MPair<x, y>``
+    contracts the per-tet tensors with the moments (see moment_tables)."""
+    mass, stiff = moment_tables()
+    lines = [
+        "// GENERATED by gen_tables.py -- do not edit.",
+        "// Quadrature-moment form of the Nedelec-2 (Volakis mixed) element integrals:",
+        "// entries = sum over tensor terms T[a][b] * (sum_alpha c_alpha * mu[alpha]),",
+        "// mu[alpha] = sum_q w_q L_q^alpha over the 11 KEAST4 points.",
+        "#pragma once",
+        "namespace emg_mtables {",
+        f"constexpr int kNumMoments = {len(MONOS)};",
+        "template <class R>",
+        "__device__ __forceinline__ void emg_moments(const R L[4], R w, R mu[kNumMoments]) {",
+    ]
+    # build monomials incrementally: degree d from degree d-1 times one L
+    name = {}
+    for i, e in enumerate(MONOS):
+        d = sum(e)
+        if d == 0:
+            lines.append(f"  const R m{i} = w;")
+        else:
+            r = max(k for k in range(4) if e[k] > 0)
+            prev = list(e)
+            prev[r] -= 1
+            lines.append(f"  const R m{i} = m{MONO_INDEX[tuple(prev)]} * L[{r}];")
+        lines.append(f"  mu[{i}] += m{i};")
+        name[e] = i
+    lines.append("}")
+    lines.append("template <int f, int s> struct MPair;")
+
+    def inner(lst):
+        # fixed evaluation order through rounding intrinsics: both triangles of a
+        # block then evaluate bitwise identically wherever the code is inlined
+        a0, c0 = lst[0]
+        e = f"emg_mul({_fmt(c0)}, mu[{a0}])"
+        for a, c in lst[1:]:
+            e = f"emg_fma({e}, {_fmt(c)}, mu[{a}])"
+        return e
+
+    for x in range(20):
+        for y in range(20):
+            lines.append(f"template <> struct MPair<{x}, {y}> {{")
+            body = "".join(f" emg_mac(acc, H[{a}][{b}], {inner(lst)});" for a, b, lst in stiff[(x, y)])
+            lines.append("  template <class A, class T, class R> __device__ __forceinline__ static void "
+                         "stiff(A &acc, const T &H, const R *mu) {" + body + " }")
+            body = "".join(f" emg_mac(acc, G[{a}][{b}], {inner(lst)});" for a, b, lst in mass[(x, y)])
+            lines.append("  template <class A, class T, class R> __device__ __forceinline__ static void "
+                         "mass(A &acc, const T &G, const R *mu) {" + body + " }")
+            lines.append("};")
+    lines.append("}  // namespace emg_mtables")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 if __name__ == "__main__":
-    emit_header(os.path.join(os.path.dirname(os.path.abspath(__file__)), "nedelec_tables.cuh"))
+    here = os.path.dirname(os.path.abspath(__file__))
+    emit_header(os.path.join(here, "nedelec_tables.cuh"))
+    emit_moment_header(os.path.join(here, "nedelec_moment_tables.cuh"))

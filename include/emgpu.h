@@ -13,9 +13,8 @@
  *   example a torch tensor). The library never allocates or frees caller
  *   memory. Host pointers are named h_*.
  * - Arrays use the reference's layouts, C-contiguous: nodes f64[3][nN],
- *   tets i32[4][nT], tet_to_edge i32[6][nT], tet_to_tri i32[4][nT],
- *   material tensors complex[3][3][nT] (only the entries the material kind
- *   needs are read, see emg_material).
+ *   tets i32[4][nT], tet_to_edge i32[6][nT], tet_to_tri i32[4][nT];
+ *   material tensors in the compact layout of their kind (emg_material).
  * - Complex numbers are interleaved (re, im) pairs of double (complex128) or
  *   float (complex64).
  * - Every function returns 0 on success or a negative EMG_E* code; the
@@ -55,18 +54,26 @@ enum {
   EMG_ST_CAPACITY = 4,   /* an entity exceeds a per-column capacity limit */
 };
 
-/* material kinds: which tensor entries are read (per tet) */
+/* material kinds and the device layout of er / ur (complex128, per tet t of
+ * the mesh, not of the assembled subset); ur may be NULL (identity) */
 enum {
-  EMG_MAT_ISO = 0,  /* er[0][0][t] (and ur[0][0][t]) scalars; ur may be NULL = 1 */
-  EMG_MAT_DIAG = 1, /* er/ur diagonals [d][d][t]; ur may be NULL = identity */
-  EMG_MAT_FULL = 2, /* all 9 entries; ur may be NULL = identity */
+  EMG_MAT_ISO = 0,  /* scalars: er[t]                               (16 B/tet) */
+  EMG_MAT_DIAG = 1, /* diagonals: er[d][t], d = 0..2                (48 B/tet) */
+  EMG_MAT_FULL = 2, /* full tensors, the reference's er[r][c][t]   (144 B/tet) */
 };
 
-/* element value precision */
+/* element value precision / form */
 enum {
-  EMG_FP64 = 0,  /* plain: everything in FP64, element values complex128 */
-  EMG_MIXED = 1, /* FP64 geometry/orientation/determinant/final sum; FP32
-                    basis-product contraction and complex64 element values */
+  EMG_FP64 = 0,  /* plain: the reference's arithmetic in FP64 (its absolute-
+                    coordinate barycentric coefficients, KEAST4 points and
+                    barycentric values, unfused), quadrature sums evaluated
+                    as per-tet moments; element values complex128 */
+  EMG_MIXED = 1, /* FP64 geometry/orientation/determinant/barycentric values
+                    and final sum; FP32 quadrature products, accumulation
+                    and contraction; element values complex64 */
+  EMG_EXACT = 2, /* exact closed-form integrals on edge-vector geometry in
+                    FP64 (free of the reference's cancellation error, so it
+                    differs from the reference by that error); complex128 */
 };
 
 /* which element values a launch produces */
@@ -78,8 +85,8 @@ enum {
 
 typedef struct {
   int kind;          /* EMG_MAT_* */
-  const void *d_er;  /* complex128 [3][3][nT] (reference layout), required */
-  const void *d_ur;  /* complex128 [3][3][nT] or NULL (identity) */
+  const void *d_er;  /* complex128, layout of `kind`, required */
+  const void *d_ur;  /* complex128, layout of `kind`, or NULL (identity) */
 } emg_material;
 
 /* Gather plan: the sparsity pattern of A plus the element-slot -> nonzero map
@@ -133,7 +140,7 @@ int emg_plan_finish(const emg_plan *plan, const int32_t *d_tet_to_edge, const in
  * reference's COO layout, value[ia*400 + 20*a + b] for reference DoF slots
  * a, b (curlcurl.py:449-455). out = EMG_OUT_K gives the reference's dataE,
  * EMG_OUT_M its dataB, EMG_OUT_LINCOMB alpha*K_e + beta*M_e. d_values is
- * complex128 for EMG_FP64 and complex64 for EMG_MIXED. Replaces
+ * complex64 for EMG_MIXED and complex128 otherwise. Replaces
  * _matrix_builder (curlcurl.py:387-456) + ned2_tet_stiff_mass (:285-380). */
 int emg_element_values(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
                        const int32_t *d_tetids, int64_t n_assy, const emg_material *mat, int precision, int out,
@@ -143,7 +150,7 @@ int emg_element_values(const double *d_nodes, int64_t n_nodes, const int32_t *d_
 /* Column gather + segmented sum: A[nnz] (complex128, CSC order of the plan)
  * = sum over element slots of alpha*V1 + beta*V2, where V1 (required) and V2
  * (optional, NULL) are element-value arrays written by emg_element_values with
- * the same precision. Deterministic (fixed summation order), no atomics.
+ * the same precision (complex64 for EMG_MIXED, complex128 otherwise). Deterministic (fixed summation order), no atomics.
  * Replaces CSCMapping.to_csc / scatter_to_csc_c16 (csc_cast.py:55-63, 162-177). */
 int emg_gather(const emg_plan *plan, const void *d_plan, const int32_t *d_indptr, const void *d_v1,
                const void *d_v2, int precision, double alpha_re, double alpha_im, double beta_re, double beta_im,

@@ -94,3 +94,37 @@ def test_dielectric_golden(precision, tol):
     g = load_json("dielectric.json")
     nodes, tets, er, ur, _ = dielectric_inputs(g)
     _summary_case(g, nodes, tets, er, ur, precision, tol)
+
+
+def test_element_values_fp64_match_reference_per_tet():
+    """Plain form reproduces the reference's arithmetic: per-tet max-entry
+    relative difference to the oracle (the reference restated) <= 1e-13 on
+    the config-0 box, whose absolute-coordinate rounding is ~1e-12."""
+    nodes, tets, er, ur = config0_inputs()
+    f = field_from(nodes, tets)
+    E, B, _ = tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64))
+    dE, dB, _ = O.tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64))
+    for mine, ref in ((np.asarray(E), dE), (np.asarray(B), dB)):
+        a = mine.reshape(-1, 400)
+        r = ref.reshape(-1, 400)
+        per = np.abs(a - r).max(axis=1) / np.abs(r).max(axis=1)
+        assert per.max() <= 1e-13, per.max()
+
+
+def test_exact_form_against_80bit_evaluation():
+    """The exact form is within 1e-13 (per tet, max-entry) of an 80-bit
+    evaluation of the exact integrals on a finer grid where the reference's
+    own rounding reaches ~1e-11."""
+    from emerge_b200 import workloads as W
+    from tests.accuracy_util import element_ld, matinv, per_tet_errors
+
+    wl = W.wr90_dielectric(n=(50, 25, 34))
+    f = wl.field
+    m = f.mesh
+    E, B, _ = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64), precision="exact")
+    ids = np.sort(np.random.default_rng(2).choice(f.ntets, 60, replace=False))
+    Ed = np.asarray(E).reshape(-1, 20, 20)[ids]
+    Bd = np.asarray(B).reshape(-1, 20, 20)[ids]
+    ref = [element_ld(m.nodes[:, m.tets[:, it]], m.tets[:, it], matinv(wl.ur[:, :, it]), wl.er[:, :, it]) for it in ids]
+    assert per_tet_errors(Ed, [r[0] for r in ref]).max() <= 1e-13
+    assert per_tet_errors(Bd, [r[1] for r in ref]).max() <= 1e-13
