@@ -22,7 +22,7 @@ EMG_OUT_LINCOMB, EMG_OUT_K, EMG_OUT_M = 0, 1, 2
 EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
-    "emg_assemble", "emg_form_sweep",
+    "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc",
 )
 
 
@@ -82,8 +82,11 @@ def lib():
     L.emg_assemble.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
                                ctypes.c_int, _D, _D, _D, _D, _P, ctypes.c_size_t, _P, _P, _P]
     L.emg_form_sweep.argtypes = [_P, _P, _P, _I64, ctypes.POINTER(_D), ctypes.c_int, _P, _I64, _P]
+    L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
+                                       ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
     for name in ("emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
-                 "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep"):
+                 "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
+                 "emg_assemble_noalloc"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

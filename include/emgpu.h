@@ -168,6 +168,24 @@ int emg_assemble(const emg_plan *plan, const void *d_plan, const int32_t *d_indp
                  int precision, double alpha_re, double alpha_im, double beta_re, double beta_im, void *d_workspace,
                  size_t workspace_bytes, void *d_A, int64_t *d_status, emg_stream_t stream);
 
+/* emg_assemble without a workspace argument, for callers that cannot
+ * allocate device memory at the call site (a plugin inside another
+ * framework's pre-reserved device pool; a latency-bound loop that must not
+ * call cudaMalloc/cudaFree, which synchronise the device). It has no
+ * counterpart in the reference. The element-value scratch is a file-scope
+ * device array of 96 MiB that every GPU loading this library holds until
+ * exit: at most 15,728 assembled tets in EMG_FP64/EMG_EXACT, 31,457 in
+ * EMG_MIXED; larger plans return EMG_ERANGE. It calls no cudaMalloc/cudaFree.
+ * The first call on a device looks the array's address up on that device
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams or
+ * threads) race and corrupt each other's results. Inputs and outputs are the
+ * caller's, as for emg_assemble. */
+int emg_assemble_noalloc(const emg_plan *plan, const void *d_plan, const int32_t *d_indptr, const double *d_nodes,
+                         int64_t n_nodes, const int32_t *d_tets, const int32_t *d_tetids, const emg_material *mat,
+                         int precision, double alpha_re, double alpha_im, double beta_re, double beta_im, void *d_A,
+                         int64_t *d_status, emg_stream_t stream);
+
 /* A_f = a_f*K + b_f*M (+ c_f*P) for nf frequencies, complex128 CSC values of
  * one pattern: K, M (and P, may be NULL) read once per call. h_coef holds
  * nf*6 doubles (a_re, a_im, b_re, b_im, c_re, c_im) per frequency; d_out
