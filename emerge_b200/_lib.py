@@ -17,6 +17,7 @@ EMG_ST_INDEX, EMG_ST_DEGENERATE, EMG_ST_CAPACITY = 1, 2, 4
 EMG_MAT_ISO, EMG_MAT_DIAG, EMG_MAT_FULL = 0, 1, 2
 EMG_FP64, EMG_MIXED, EMG_EXACT = 0, 1, 2
 EMG_OUT_LINCOMB, EMG_OUT_K, EMG_OUT_M = 0, 1, 2
+EMG_LAYOUT_COO, EMG_LAYOUT_PACKED = 0, 1
 
 # every symbol include/emgpu.h declares
 EXPORTS = (
@@ -43,7 +44,9 @@ class Plan(ctypes.Structure):
         ("n_tris", ctypes.c_int64), ("n_ent", ctypes.c_int64), ("n_items", ctypes.c_int64), ("N", ctypes.c_int64),
         ("nnz", ctypes.c_int64), ("max_col", ctypes.c_int64), ("off_ent_ptr", ctypes.c_size_t),
         ("off_item", ctypes.c_size_t), ("off_item_pos", ctypes.c_size_t), ("off_ent_cnt", ctypes.c_size_t),
-        ("plan_bytes", ctypes.c_size_t), ("workspace_bytes", ctypes.c_size_t),
+        ("off_contrib", ctypes.c_size_t), ("off_posoff", ctypes.c_size_t), ("off_pidx", ctypes.c_size_t),
+        ("plan_bytes", ctypes.c_size_t),
+        ("workspace_bytes", ctypes.c_size_t),
     ]
 
 
@@ -72,11 +75,12 @@ def lib():
     L.emg_status_reset.argtypes = [_P, _P]
     L.emg_status_read.argtypes = [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P]
     L.emg_plan_init.argtypes = [_I64, _I64, _I64, _I64, ctypes.POINTER(Plan)]
-    L.emg_plan_build.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _P, _P, _P, _P, _P]
+    L.emg_plan_build.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _P, _P, _P, _P, _P, _P]
     L.emg_plan_finish.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _P, _P, _P, _P, _P]
     L.emg_element_values.argtypes = [_P, _I64, _P, _I64, _P, _I64, ctypes.POINTER(Material), ctypes.c_int,
-                                     ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
-    L.emg_gather.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _P, ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
+                                     ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
+    L.emg_gather.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _P,
+                             _P, _P]
     L.emg_assemble_workspace_size.argtypes = [_I64, ctypes.c_int]
     L.emg_assemble_workspace_size.restype = ctypes.c_size_t
     L.emg_assemble.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),

@@ -217,8 +217,8 @@ class ElemValues:
         m.reset_status()
         L.check(L.lib().emg_element_values(
             L.ptr(m.nodes), m.n_nodes, L.ptr(m.tets), m.n_tets, L.ptr(m.tetids), m.n_assy, L.ctypes.byref(mat),
-            job.precision, L.EMG_OUT_K if self.which == "K" else L.EMG_OUT_M, 0.0, 0.0, 0.0, 0.0, L.ptr(out),
-            L.ptr(m.status), L.stream_handle(m.device)))
+            job.precision, L.EMG_OUT_K if self.which == "K" else L.EMG_OUT_M, L.EMG_LAYOUT_COO, 0.0, 0.0, 0.0, 0.0,
+            L.ptr(out), L.ptr(m.status), L.stream_handle(m.device)))
         m.check_status()
         return out
 
@@ -308,8 +308,8 @@ class GpuCSCMapping:
         self.d_indptr = torch.empty(self.N + 1, dtype=torch.int32, device=m.device)
         t2e, t2t = m.topology()
         st = L.stream_handle(m.device)
-        L.check(lib.emg_plan_build(L.ctypes.byref(plan), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids), L.ptr(self.d_plan),
-                                   L.ptr(ws), L.ptr(self.d_indptr), L.ptr(m.status), st))
+        L.check(lib.emg_plan_build(L.ctypes.byref(plan), L.ptr(m.tets), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids),
+                                   L.ptr(self.d_plan), L.ptr(ws), L.ptr(self.d_indptr), L.ptr(m.status), st))
         del ws
         self.nnz = int(plan.nnz)
         self.d_indices = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=m.device)
@@ -363,7 +363,7 @@ class GpuCSCMapping:
         if out is None:
             out = torch.empty(max(self.nnz, 1), dtype=torch.complex128, device=self.device)
         L.check(L.lib().emg_gather(L.ctypes.byref(self.plan), L.ptr(self.d_plan), L.ptr(self.d_indptr), L.ptr(values),
-                                   None, precision, 1.0, 0.0, 0.0, 0.0, L.ptr(out), None,
+                                   None, precision, L.EMG_LAYOUT_COO, 1.0, 0.0, 0.0, 0.0, L.ptr(out), None,
                                    L.stream_handle(self.device)))
         return out
 

@@ -20,18 +20,18 @@ const char *last_error() { return g_err; }
 namespace {
 __global__ void k_probe() {}
 
-int launch_element(const ElemArgs &a, int kind, int precision, int out, cudaStream_t s) {
+int launch_element(const ElemArgs &a, int kind, int precision, int layout, cudaStream_t s) {
   if (kind < EMG_MAT_ISO || kind > EMG_MAT_FULL) return fail(EMG_EINVAL, "bad material kind %d", kind);
   switch (precision * 3 + kind) {
-    case 0: return launch_element_0_0(a, out, s);
-    case 1: return launch_element_0_1(a, out, s);
-    case 2: return launch_element_0_2(a, out, s);
-    case 3: return launch_element_1_0(a, out, s);
-    case 4: return launch_element_1_1(a, out, s);
-    case 5: return launch_element_1_2(a, out, s);
-    case 6: return launch_element_2_0(a, out, s);
-    case 7: return launch_element_2_1(a, out, s);
-    case 8: return launch_element_2_2(a, out, s);
+    case 0: return launch_element_0_0(a, layout, s);
+    case 1: return launch_element_0_1(a, layout, s);
+    case 2: return launch_element_0_2(a, layout, s);
+    case 3: return launch_element_1_0(a, layout, s);
+    case 4: return launch_element_1_1(a, layout, s);
+    case 5: return launch_element_1_2(a, layout, s);
+    case 6: return launch_element_2_0(a, layout, s);
+    case 7: return launch_element_2_1(a, layout, s);
+    case 8: return launch_element_2_2(a, layout, s);
   }
   return fail(EMG_EINVAL, "bad precision %d", precision);
 }
@@ -78,7 +78,8 @@ int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tri
   if (!p) return fail(EMG_EINVAL, "null plan");
   if (n_tets < 0 || n_assy < 0 || n_edges < 0 || n_tris < 0) return fail(EMG_EINVAL, "negative size");
   if (n_assy > n_tets) return fail(EMG_EINVAL, "n_assy (%lld) > n_tets (%lld)", (long long)n_assy, (long long)n_tets);
-  if (n_assy > (int64_t)(INT32_MAX / 400) || n_tets > INT32_MAX || 2 * (n_edges + n_tris) >= INT32_MAX)
+  if (n_assy > (int64_t)(INT32_MAX / 400) || n_tets > INT32_MAX || 2 * (n_edges + n_tris) >= INT32_MAX ||
+      n_assy * 20 > (int64_t)INT32_MAX / 10)
     return fail(EMG_ERANGE, "mesh too large for 32-bit indexing (n_assy=%lld)", (long long)n_assy);
   memset(p, 0, sizeof(*p));
   p->n_tets = n_tets;
@@ -93,11 +94,12 @@ int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tri
   return EMG_OK;
 }
 
-int emg_plan_build(emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids, void *d_plan,
-                   void *d_ws, int32_t *d_indptr, int64_t *d_status, emg_stream_t stream) {
+int emg_plan_build(emg_plan *p, const int32_t *d_tets, const int32_t *d_t2e, const int32_t *d_t2t,
+                   const int32_t *d_tetids, void *d_plan, void *d_ws, int32_t *d_indptr, int64_t *d_status,
+                   emg_stream_t stream) {
   if (!p || !d_plan || !d_ws || !d_indptr || !d_status) return fail(EMG_EINVAL, "null pointer");
-  if (p->n_assy > 0 && (!d_t2e || !d_t2t)) return fail(EMG_EINVAL, "null topology pointer");
-  return plan_build(p, d_t2e, d_t2t, d_tetids, d_plan, d_ws, d_indptr, d_status, S(stream));
+  if (p->n_assy > 0 && (!d_tets || !d_t2e || !d_t2t)) return fail(EMG_EINVAL, "null topology pointer");
+  return plan_build(p, d_tets, d_t2e, d_t2t, d_tetids, d_plan, d_ws, d_indptr, d_status, S(stream));
 }
 
 int emg_plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids,
@@ -110,30 +112,39 @@ int emg_plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2
 
 int emg_element_values(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
                        const int32_t *d_tetids, int64_t n_assy, const emg_material *mat, int precision, int out,
-                       double ar, double ai, double br, double bi, void *d_values, int64_t *d_status,
+                       int layout, double ar, double ai, double br, double bi, void *d_values, int64_t *d_status,
                        emg_stream_t stream) {
   if (!mat || !mat->d_er) return fail(EMG_EINVAL, "material with a null er pointer");
   if (n_assy < 0 || n_tets < 0 || n_nodes < 0) return fail(EMG_EINVAL, "negative size");
   if (n_assy > 0 && (!d_nodes || !d_tets || !d_values)) return fail(EMG_EINVAL, "null pointer");
   if (n_assy > (int64_t)(INT32_MAX / 400)) return fail(EMG_ERANGE, "too many tets (%lld)", (long long)n_assy);
   if (!d_tetids && n_assy > n_tets) return fail(EMG_EINVAL, "n_assy > n_tets without tetids");
+  if (out == EMG_OUT_K) {
+    ar = 1.0, ai = 0.0, br = 0.0, bi = 0.0;
+  } else if (out == EMG_OUT_M) {
+    ar = 0.0, ai = 0.0, br = 1.0, bi = 0.0;
+  } else if (out != EMG_OUT_LINCOMB) {
+    return fail(EMG_EINVAL, "bad output selector %d", out);
+  }
   ElemArgs a{d_nodes, n_nodes, d_tets, n_tets, d_tetids, n_assy, mat->d_er, mat->d_ur, ar, ai, br, bi, d_values,
              d_status};
-  return launch_element(a, mat->kind, precision, out, S(stream));
+  return launch_element(a, mat->kind, precision, layout, S(stream));
 }
 
 int emg_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_v1, const void *d_v2,
-               int precision, double ar, double ai, double br, double bi, void *d_A, int64_t *d_status,
+               int precision, int layout, double ar, double ai, double br, double bi, void *d_A, int64_t *d_status,
                emg_stream_t stream) {
   if (!p || !d_plan || !d_indptr) return fail(EMG_EINVAL, "null pointer");
   if (p->nnz > 0 && (!d_v1 || !d_A)) return fail(EMG_EINVAL, "null value pointer");
-  return launch_gather(p, d_plan, d_indptr, d_v1, d_v2, precision, ar, ai, br, bi, d_A, d_status, S(stream));
+  if (layout == EMG_LAYOUT_PACKED && d_v2) return fail(EMG_EINVAL, "the packed layout takes one value array");
+  return launch_gather(p, d_plan, d_indptr, d_v1, d_v2, precision, layout, ar, ai, br, bi, d_A, d_status,
+                       S(stream));
 }
 
 size_t emg_assemble_workspace_size(int64_t n_assy, int precision) {
   if (n_assy < 0) return 0;
   if (precision < EMG_FP64 || precision > EMG_EXACT) return 0;
-  return (size_t)n_assy * 400 * (values_fp32(precision) ? 8 : 16);
+  return (size_t)n_assy * 210 * (values_fp32(precision) ? 8 : 16);
 }
 
 int emg_assemble(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const double *d_nodes,
@@ -145,9 +156,10 @@ int emg_assemble(const emg_plan *p, const void *d_plan, const int32_t *d_indptr,
     return fail(EMG_EINVAL, "workspace too small: %zu < %zu", ws_bytes,
                 emg_assemble_workspace_size(p->n_assy, precision));
   int rc = emg_element_values(d_nodes, n_nodes, d_tets, p->n_tets, d_tetids, p->n_assy, mat, precision,
-                              EMG_OUT_LINCOMB, ar, ai, br, bi, d_ws, d_status, stream);
+                              EMG_OUT_LINCOMB, EMG_LAYOUT_PACKED, ar, ai, br, bi, d_ws, d_status, stream);
   if (rc) return rc;
-  return emg_gather(p, d_plan, d_indptr, d_ws, nullptr, precision, 1.0, 0.0, 0.0, 0.0, d_A, d_status, stream);
+  return emg_gather(p, d_plan, d_indptr, d_ws, nullptr, precision, EMG_LAYOUT_PACKED, 1.0, 0.0, 0.0, 0.0, d_A,
+                    d_status, stream);
 }
 
 int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,

@@ -36,6 +36,32 @@ inline int grid_for(int64_t n, int threads) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// canonical edge index of rank pair r1 != r2 in (0,1),(0,2),(0,3),(1,2),(1,3),(2,3)
+__host__ __device__ __forceinline__ int canon_edge(int a, int b) {
+  int r1 = a < b ? a : b, r2 = a < b ? b : a;
+  return r1 == 0 ? r2 - 1 : (r1 == 1 ? r2 + 1 : 5);
+}
+
+// Canonical DoF (0..19) of reference DoF slot r of a tet whose vertex ranks
+// are packed 2 bits per local vertex: edge slots use local vertex pairs
+// (0,1),(0,2),(0,3),(1,2),(3,1),(2,3) and face slots miss vertex 3,1,2,0
+// (mesh3d.py:760-761); canonical edges are rank pairs, canonical faces are
+// numbered 3 - (rank of the missing vertex).
+__host__ __device__ __forceinline__ int canon_dof(int ranks, int r) {
+  if (r < 12) {
+    const int e = r < 6 ? r : r - 6;
+    const int u = e < 3 ? 0 : (e == 3 ? 1 : (e == 4 ? 3 : 2));
+    const int v = e < 3 ? e + 1 : (e == 3 ? 2 : (e == 4 ? 1 : 3));
+    return (r < 6 ? 0 : 6) + canon_edge((ranks >> (2 * u)) & 3, (ranks >> (2 * v)) & 3);
+  }
+  const int f = r < 16 ? r - 12 : r - 16;
+  const int miss = f == 0 ? 3 : (f == 1 ? 1 : (f == 2 ? 2 : 0));
+  return (r < 16 ? 12 : 16) + 3 - ((ranks >> (2 * miss)) & 3);
+}
+
+// index of canonical pair (x, y), x <= y, in the packed upper triangle
+__host__ __device__ __forceinline__ int packed_index(int x, int y) { return x * (41 - x) / 2 + (y - x); }
+
 // status word: [0] flags (EMG_ST_*), [1] smallest offending index
 __device__ __forceinline__ void flag(int64_t *st, int64_t bit, int64_t index) {
   if (st) {
@@ -52,7 +78,7 @@ struct __align__(16) Item {
   int32_t ia;
   uint8_t slot;
   uint8_t pos[10];
-  uint8_t pad;
+  uint8_t ranks;  // vertex ranks of the tet by global node id: 2 bits per local vertex
 };
 static_assert(sizeof(Item) == 16, "item record must be 16 bytes");
 
@@ -70,9 +96,21 @@ struct ElemArgs {
   int64_t *st;
 };
 
+// Gather chunks: a warp owns CHUNK consecutive entities of one kind. Their
+// items are contiguous in the plan and their first-DoF (second-DoF) columns
+// are consecutive, so each chunk's output is two contiguous runs of A.
+constexpr int CHUNK = 8;
+constexpr int CHUNK_MAX_POS = 1024;   // positions per run of a chunk (plan capacity)
+constexpr int CHUNK_MAX_ITEMS = 1023; // items per chunk (10-bit item index)
+
+__host__ __device__ __forceinline__ int64_t n_edge_chunks(int64_t E) { return (E + CHUNK - 1) / CHUNK; }
+__host__ __device__ __forceinline__ int64_t n_chunks(int64_t E, int64_t F) {
+  return n_edge_chunks(E) + (F + CHUNK - 1) / CHUNK;
+}
+
 // element kernel launchers, one translation unit per (form, material kind);
 // form 0 = reference-faithful FP64, 1 = mixed, 2 = exact closed form
-#define EMG_DECLARE_ELEM(F, K) int launch_element_##F##_##K(const ElemArgs &a, int out, cudaStream_t s);
+#define EMG_DECLARE_ELEM(F, K) int launch_element_##F##_##K(const ElemArgs &a, int layout, cudaStream_t s);
 EMG_DECLARE_ELEM(0, 0)
 EMG_DECLARE_ELEM(0, 1)
 EMG_DECLARE_ELEM(0, 2)
@@ -89,15 +127,16 @@ inline bool values_fp32(int precision) { return precision == EMG_MIXED; }
 // plan.cu
 size_t plan_workspace_bytes(const emg_plan *p);
 size_t plan_layout(emg_plan *p);
-int plan_build(emg_plan *p, const int32_t *t2e, const int32_t *t2t, const int32_t *tetids, void *d_plan, void *d_ws,
-               int32_t *indptr, int64_t *st, cudaStream_t s);
+int plan_build(emg_plan *p, const int32_t *tets, const int32_t *t2e, const int32_t *t2t, const int32_t *tetids,
+               void *d_plan, void *d_ws, int32_t *indptr, int64_t *st, cudaStream_t s);
 int plan_finish(const emg_plan *p, const int32_t *t2e, const int32_t *t2t, const int32_t *tetids, void *d_plan,
                 const int32_t *indptr, int32_t *indices, int64_t *st, cudaStream_t s);
 int status_reset(int64_t *st, cudaStream_t s);
 
 // gather.cu
 int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *indptr, const void *v1, const void *v2,
-                  int precision, double ar, double ai, double br, double bi, void *A, int64_t *st, cudaStream_t s);
+                  int precision, int layout, double ar, double ai, double br, double bi, void *A, int64_t *st,
+                  cudaStream_t s);
 int launch_form_sweep(const void *K, const void *M, const void *P, int64_t nnz, const double *coef, int nf,
                       void *out, int64_t stride, cudaStream_t s);
 

@@ -120,11 +120,6 @@ struct Geo {
   uint64_t inv;    // nibble c (0..9 canonical entity) -> reference entity slot (0..9)
 };
 
-// canonical edge index of rank pair r1 < r2 in (0,1),(0,2),(0,3),(1,2),(1,3),(2,3)
-__device__ __forceinline__ int canon_edge(int a, int b) {
-  int r1 = min(a, b), r2 = max(a, b);
-  return r1 == 0 ? r2 - 1 : (r1 == 1 ? r2 + 1 : 5);
-}
 
 // Barycentric coefficients exactly as the reference forms them
 // (tet_coefficients, curlcurl.py:127-214): 24-term determinant and signed
@@ -314,7 +309,9 @@ __device__ __forceinline__ bool ref_geometry(const double X[3][4], const int64_t
   G.inv = inv;
 #pragma unroll
   for (int i = 0; i < NMOM; ++i) mu[i] = (R)0;
-#pragma unroll
+  // rolled on purpose: the kernel is instruction-fetch bound, and the point
+  // loop body is the same for all 11 points
+#pragma unroll 1
   for (int q = 0; q < 11; ++q) {
     const double p1 = kDP[1][q], p2 = kDP[2][q], p3 = kDP[3][q], p4 = kDP[4][q];
     double xq[3];
@@ -576,7 +573,7 @@ __device__ __forceinline__ void do_row(const Tensors<KIND, R> &T, const R *mu, d
                                   std::make_integer_sequence<int, 20>{});
   __syncwarp();
   // cooperative, coalesced write of the warp's 32 rows (each 20 contiguous values)
-#pragma unroll 4
+#pragma unroll 1
   for (int it = 0; it < 20; ++it) {
     int e = it * 32 + lane;
     int r = e / 20, c = e - r * 20;
@@ -596,12 +593,86 @@ __device__ __forceinline__ void all_rows(const Tensors<KIND, R> &T, const R *mu,
   (do_row<FORM, KIND, R, Xs>(T, mu, sig, cK, cM, inv, active, ia, stage, out), ...);
 }
 
-template <int FORM, int KIND, int OUT>
+// ---- packed canonical layout: value[ia*210 + packed_index(x, y)], x <= y,
+// canonical DoFs. Each unique pair is computed once; canonical row X (its
+// 20 - X upper-triangle entries) is staged in shared memory and the warp
+// writes its 32 row segments as contiguous runs.
+template <int x, int y, int FORM, int KIND, typename R>
+__device__ __forceinline__ void compute_store_packed(const Tensors<KIND, R> &T, const R *mu, double sig,
+                                                     const CR<R> &cK, const CR<R> &cM, uint64_t inv,
+                                                     typename StoreT<R>::T *row) {
+  using ST = typename StoreT<R>::T;
+  ST v;
+  if constexpr (KIND == EMG_MAT_ISO) {
+    R k0, m0;
+    entry<x, y, FORM, KIND, R>(T, mu, sig, k0, m0);
+    v.x = cfma(cK.re, k0, cmul_rn(cM.re, m0));
+    v.y = cfma(cK.im, k0, cmul_rn(cM.im, m0));
+  } else {
+    CR<R> k, m;
+    if constexpr (KIND == EMG_MAT_DIAG) {
+      entry<x, y, FORM, KIND, R>(T, mu, sig, k, m);
+    } else {
+      // first = the DoF with the lower reference index (curlcurl.py:358-376)
+      if (ref_dof(inv, x) <= ref_dof(inv, y)) {
+        entry<x, y, FORM, KIND, R>(T, mu, sig, k, m);
+      } else {
+        entry<y, x, FORM, KIND, R>(T, mu, sig, k, m);
+      }
+    }
+    v.x = cfma(cK.re, k.re, cfma(-cK.im, k.im, cfma(cM.re, m.re, cmul_rn(-cM.im, m.im))));
+    v.y = cfma(cK.re, k.im, cfma(cK.im, k.re, cfma(cM.re, m.im, cmul_rn(cM.im, m.re))));
+  }
+  row[y - x] = v;
+}
+
+template <int x, int FORM, int KIND, typename R, int... Ds>
+__device__ __forceinline__ void compute_row_packed(const Tensors<KIND, R> &T, const R *mu, double sig,
+                                                   const CR<R> &cK, const CR<R> &cM, uint64_t inv,
+                                                   typename StoreT<R>::T *row, std::integer_sequence<int, Ds...>) {
+  (compute_store_packed<x, x + Ds, FORM, KIND, R>(T, mu, sig, cK, cM, inv, row), ...);
+}
+
+template <int FORM, int KIND, typename R, int X>
+__device__ __forceinline__ void do_row_packed(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                              const CR<R> &cM, uint64_t inv, bool active, int ia,
+                                              typename StoreT<R>::T *stage, typename StoreT<R>::T *out) {
+  constexpr int W = 20 - X;
+  const int lane = threadIdx.x & 31;
+  if (active)
+    compute_row_packed<X, FORM, KIND, R>(T, mu, sig, cK, cM, inv, stage + lane * W,
+                                         std::make_integer_sequence<int, W>{});
+  __syncwarp();
+#pragma unroll 1
+  for (int it = 0; it < W; ++it) {
+    const int e = it * 32 + lane;
+    const int r = e / W, c = e - r * W;
+    const int ia_r = __shfl_sync(0xffffffffu, ia, r);
+    const bool act_r = __shfl_sync(0xffffffffu, (int)active, r);
+    if (act_r) out[(int64_t)ia_r * 210 + packed_index(X, X) + c] = stage[r * W + c];
+  }
+  __syncwarp();
+}
+
+template <int FORM, int KIND, typename R, int... Xs>
+__device__ __forceinline__ void all_rows_packed(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                                const CR<R> &cM, uint64_t inv, bool active, int ia,
+                                                typename StoreT<R>::T *stage, typename StoreT<R>::T *out,
+                                                std::integer_sequence<int, Xs...>) {
+  (do_row_packed<FORM, KIND, R, Xs>(T, mu, sig, cK, cM, inv, active, ia, stage, out), ...);
+}
+
+// LAYOUT 0: the reference's COO block [ia][a][b] (400 values, each entry
+//           computed in both of its rows);
+// LAYOUT 1: the packed canonical upper triangle [ia][210] (the assembly
+//           path, each unique entry computed once)
+template <int FORM, int KIND, int LAYOUT>
 __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
   using R = typename FormReal<FORM>::T;
   using ST = typename StoreT<R>::T;
-  __shared__ ST stage_all[ELEM_WARPS][32 * 20];
-  ST *stage = stage_all[threadIdx.x >> 5];
+  constexpr int STAGE = 20;  // values per lane
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  ST *stage = reinterpret_cast<ST *>(stage_raw) + (threadIdx.x >> 5) * (32 * STAGE);
   ST *out = reinterpret_cast<ST *>(a.out);
   const int64_t ia64 = (int64_t)blockIdx.x * ELEM_THREADS + threadIdx.x;
   bool active = ia64 < a.nA;
@@ -644,14 +715,7 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
       } else {
         sig = G.sig;
         inv = G.inv;
-        C64 alpha{a.ar, a.ai}, beta{a.br, a.bi};
-        if (OUT == EMG_OUT_K) {
-          alpha = {1.0, 0.0};
-          beta = {0.0, 0.0};
-        } else if (OUT == EMG_OUT_M) {
-          alpha = {0.0, 0.0};
-          beta = {1.0, 0.0};
-        }
+        const C64 alpha{a.ar, a.ai}, beta{a.br, a.bi};
         if constexpr (KIND == EMG_MAT_ISO) {
           C64 eps = ld_c64(a.er, it);
           C64 minv = a.ur ? crecip(ld_c64(a.ur, it)) : C64{1.0, 0.0};
@@ -679,24 +743,35 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
       }
     }
   }
-  all_rows<FORM, KIND, R>(T, mu, sig, cK, cM, inv, active, ia, stage, out, std::make_integer_sequence<int, 20>{});
+  if constexpr (LAYOUT == 0) {
+    all_rows<FORM, KIND, R>(T, mu, sig, cK, cM, inv, active, ia, stage, out, std::make_integer_sequence<int, 20>{});
+  } else {
+    all_rows_packed<FORM, KIND, R>(T, mu, sig, cK, cM, inv, active, ia, stage, out,
+                                   std::make_integer_sequence<int, 20>{});
+  }
 }
 
-template <int FORM, int KIND, int OUT>
+template <int FORM, int KIND, int LAYOUT>
 int launch_element_t(const ElemArgs &a, cudaStream_t s) {
+  using ST = typename StoreT<typename FormReal<FORM>::T>::T;
+  constexpr size_t smem = (size_t)ELEM_WARPS * 32 * 20 * sizeof(ST);
+  static bool configured = false;  // benign race: every thread sets the same value
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_element<FORM, KIND, LAYOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return fail(EMG_ECUDA, "cudaFuncSetAttribute(k_element): %s", cudaGetErrorString(e));
+    configured = true;
+  }
   if (a.nA == 0) return EMG_OK;
-  k_element<FORM, KIND, OUT><<<grid_for(a.nA, ELEM_THREADS), ELEM_THREADS, 0, s>>>(a);
+  k_element<FORM, KIND, LAYOUT><<<grid_for(a.nA, ELEM_THREADS), ELEM_THREADS, smem, s>>>(a);
   return launch_check("k_element");
 }
 
 template <int FORM, int KIND>
-int launch_element_k(const ElemArgs &a, int out, cudaStream_t s) {
-  switch (out) {
-    case EMG_OUT_LINCOMB: return launch_element_t<FORM, KIND, EMG_OUT_LINCOMB>(a, s);
-    case EMG_OUT_K: return launch_element_t<FORM, KIND, EMG_OUT_K>(a, s);
-    case EMG_OUT_M: return launch_element_t<FORM, KIND, EMG_OUT_M>(a, s);
-  }
-  return fail(EMG_EINVAL, "bad output selector %d", out);
+int launch_element_k(const ElemArgs &a, int layout, cudaStream_t s) {
+  if (layout == EMG_LAYOUT_COO) return launch_element_t<FORM, KIND, 0>(a, s);
+  if (layout == EMG_LAYOUT_PACKED) return launch_element_t<FORM, KIND, 1>(a, s);
+  return fail(EMG_EINVAL, "bad layout %d", layout);
 }
 
 }  // namespace

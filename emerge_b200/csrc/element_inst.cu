@@ -14,7 +14,7 @@
 #define EMG_CAT(a, b, c) EMG_CAT2(a, b, c)
 
 namespace emg {
-int EMG_CAT(launch_element_, EMG_FORM, EMG_KIND)(const ElemArgs &a, int out, cudaStream_t s) {
-  return launch_element_k<EMG_FORM, EMG_KIND>(a, out, s);
+int EMG_CAT(launch_element_, EMG_FORM, EMG_KIND)(const ElemArgs &a, int layout, cudaStream_t s) {
+  return launch_element_k<EMG_FORM, EMG_KIND>(a, layout, s);
 }
 }  // namespace emg

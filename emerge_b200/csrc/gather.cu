@@ -12,8 +12,6 @@ struct C64 {
   double re, im;
 };
 
-constexpr int GATHER_WARPS = 8;
-constexpr int COL_CAP = 160;  // column entries buffered in shared memory per column
 
 template <typename R>
 __device__ __forceinline__ C64 load_val(const void *p, int64_t idx) {
@@ -26,71 +24,137 @@ __device__ __forceinline__ C64 load_val(const void *p, int64_t idx) {
   }
 }
 
+// Pull gather (every layout). A warp owns one entity chunk (CHUNK consecutive
+// entities of one kind, see common.cuh); its two output runs are contiguous.
+// Lane l owns positions l, l+32, ... of the runs: it reads the position's
+// contribution list from the plan (item of the chunk, element row), sums the
+// contributing element values in that fixed order (items ascending, so tets
+// ascending), and writes the first-DoF and second-DoF entries once. No shared
+// memory, no atomics; each nonzero is produced by exactly one lane.
+constexpr int PG_WARPS = 8;
+
+// element slots (row r, column a0) and (row r, column a1) of the reference COO
+// block: the item's contributions to its entity's two columns
+template <typename R>
+__device__ __forceinline__ void load_coo_pair(const void *v, int ia, int slot, int r, C64 &u0, C64 &u1) {
+  const int a0 = slot < 6 ? slot : 12 + (slot - 6);
+  const int a1 = slot < 6 ? slot + 6 : 16 + (slot - 6);
+  const int64_t base = (int64_t)ia * 400 + r * 20;
+  u0 = load_val<R>(v, base + a0);
+  u1 = load_val<R>(v, base + a1);
+}
+
+struct ChunkMeta {
+  int32_t I0, I1, A0, A1, Lsum;
+  int64_t hbase;
+};
+
+// Processing position g -> chunk. Edge chunks and face chunks are each sorted
+// by their entities' lowest node; interleaving them in proportion keeps the
+// edge and face chunks of one mesh region together, so the element values of
+// that region's tets are read while still in L2.
+__device__ __forceinline__ int64_t chunk_at(int64_t g, int64_t nec, int64_t nch) {
+  const int64_t ce0 = (g * nec) / nch, ce1 = ((g + 1) * nec) / nch;
+  return ce1 > ce0 ? ce0 : nec + (g - ce0);
+}
+
+__device__ __forceinline__ bool chunk_meta(const int32_t *ent_ptr, const int32_t *indptr, int64_t E, int64_t F,
+                                           int64_t g, ChunkMeta &m) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nec = n_edge_chunks(E);
+  const int64_t nch = n_chunks(E, F);
+  if (g >= nch) return false;
+  const int64_t chunk = chunk_at(g, nec, nch);
+  const bool edges = chunk < nec;
+  const int64_t x0 = edges ? chunk * CHUNK : E + (chunk - nec) * CHUNK;
+  const int nx = (int)min((int64_t)CHUNK, (edges ? E : E + F) - x0);
+  const int64_t cb0 = edges ? x0 : E + x0;          // first-DoF column of x0 (faces: 2E + (x0 - E))
+  const int64_t cb1 = edges ? x0 + E : E + F + x0;  // second-DoF column of x0
+  int32_t meta = 0;
+  if (lane == 0) meta = ent_ptr[x0];
+  else if (lane == 1) meta = ent_ptr[x0 + nx];
+  else if (lane == 2) meta = indptr[cb0];
+  else if (lane == 3) meta = indptr[cb0 + nx];
+  else if (lane == 4) meta = indptr[cb1];
+  else if (lane == 5) meta = edges ? 0 : indptr[E];
+  else if (lane == 6) meta = edges ? 0 : indptr[2 * E];
+  m.I0 = __shfl_sync(0xffffffffu, meta, 0);
+  m.I1 = __shfl_sync(0xffffffffu, meta, 1);
+  m.A0 = __shfl_sync(0xffffffffu, meta, 2);
+  m.Lsum = __shfl_sync(0xffffffffu, meta, 3) - m.A0;
+  m.A1 = __shfl_sync(0xffffffffu, meta, 4);
+  const int32_t cE = __shfl_sync(0xffffffffu, meta, 5), c2E = __shfl_sync(0xffffffffu, meta, 6);
+  m.hbase = edges ? (int64_t)m.A0 : (int64_t)cE + (m.A0 - c2E);
+  return true;
+}
+
+// reference COO layout (any COO data of this field's slot layout)
 template <typename R, bool TWO>
-__global__ void __launch_bounds__(GATHER_WARPS * 32)
-    k_gather(const int32_t *ent_ptr, const Item *items, const uint32_t *ent_cnt, int64_t n_ent, int64_t E, int64_t F,
-             const int32_t *indptr, const void *v1, const void *v2, double ar, double ai, double br, double bi,
-             double2 *A, int64_t *st) {
-  __shared__ double2 buf_all[GATHER_WARPS][2][COL_CAP];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t x = (int64_t)blockIdx.x * GATHER_WARPS + w;
-  if (x >= n_ent) return;
-  const uint32_t cnt = ent_cnt[x];
-  const int ne = (int)(cnt & 0xffffu), nf = (int)(cnt >> 16);
-  const int L = 2 * (ne + nf);
-  const bool is_edge = x < E;
-  const int64_t c0 = is_edge ? x : E + x;
-  const int64_t c1 = is_edge ? x + E : E + F + x;
-  const int64_t s0 = indptr[c0], s1 = indptr[c1];
-  const bool in_smem = L <= COL_CAP;
-  double2 *b0 = in_smem ? buf_all[w][0] : A + s0;
-  double2 *b1 = in_smem ? buf_all[w][1] : A + s1;
-  for (int i = lane; i < L; i += 32) {
-    b0[i] = make_double2(0.0, 0.0);
-    b1[i] = make_double2(0.0, 0.0);
-  }
-  __syncwarp();
-  const int32_t ib = ent_ptr[x], ie = ent_ptr[x + 1];
-  // row r of an element block -> entity slot and block offset in the column
-  const int r = lane;
-  const int sl = r < 6 ? r : (r < 12 ? r - 6 : (r < 16 ? r - 6 : r - 10));
-  const int off = r < 6 ? 0 : (r < 12 ? ne : (r < 16 ? 2 * ne : 2 * ne + nf));
-  for (int32_t k = ib; k < ie; ++k) {
-    const Item rec = items[k];
-    if (r < 20) {
-      const int s = rec.slot;
-      const int a0 = s < 6 ? s : 12 + (s - 6);
-      const int a1 = s < 6 ? s + 6 : 16 + (s - 6);
-      const int64_t base = (int64_t)rec.ia * 400;
-      C64 u0 = load_val<R>(v1, base + a0 * 20 + r);
-      C64 u1 = load_val<R>(v1, base + a1 * 20 + r);
-      C64 y0, y1;
-      y0 = {ar * u0.re - ai * u0.im, ar * u0.im + ai * u0.re};
-      y1 = {ar * u1.re - ai * u1.im, ar * u1.im + ai * u1.re};
+__global__ void __launch_bounds__(PG_WARPS * 32)
+    k_gather_coo(const int32_t *ent_ptr, const Item *items, const uint16_t *contrib, const uint16_t *posoff,
+                 int64_t E, int64_t F, const int32_t *indptr, const void *v1, const void *v2, double ar, double ai,
+                 double br, double bi, double2 *A) {
+  const int lane = threadIdx.x & 31;
+  ChunkMeta m;
+  if (!chunk_meta(ent_ptr, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
+  const int total = 20 * (m.I1 - m.I0);
+  const uint16_t *clist = contrib + (int64_t)20 * m.I0;
+  const Item *it = items + m.I0;
+  for (int p = lane; p < m.Lsum; p += 32) {
+    const int o0 = posoff[m.hbase + p];
+    const int o1 = min(p + 1 < m.Lsum ? (int)posoff[m.hbase + p + 1] : total, total);
+    double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
+    for (int k = o0; k < o1; ++k) {
+      const uint32_t c = clist[k];
+      if ((int)(c >> 5) >= m.I1 - m.I0) continue;  // only a plan whose build was flagged can hold this
+      const uint4 rec = __ldg(reinterpret_cast<const uint4 *>(it + (c >> 5)));
+      const int r = (int)(c & 31u);
+      C64 u0, u1;
+      load_coo_pair<R>(v1, (int)rec.x, (int)(rec.y & 0xffu), r, u0, u1);
+      s0r += ar * u0.re - ai * u0.im;
+      s0i += ar * u0.im + ai * u0.re;
+      s1r += ar * u1.re - ai * u1.im;
+      s1i += ar * u1.im + ai * u1.re;
       if (TWO) {
-        C64 w0 = load_val<R>(v2, base + a0 * 20 + r);
-        C64 w1 = load_val<R>(v2, base + a1 * 20 + r);
-        y0.re += br * w0.re - bi * w0.im;
-        y0.im += br * w0.im + bi * w0.re;
-        y1.re += br * w1.re - bi * w1.im;
-        y1.im += br * w1.im + bi * w1.re;
+        C64 t0, t1;
+        load_coo_pair<R>(v2, (int)rec.x, (int)(rec.y & 0xffu), r, t0, t1);
+        s0r += br * t0.re - bi * t0.im;
+        s0i += br * t0.im + bi * t0.re;
+        s1r += br * t1.re - bi * t1.im;
+        s1i += br * t1.im + bi * t1.re;
       }
-      const int p = off + rec.pos[sl];
-      double2 t0 = b0[p], t1 = b1[p];
-      t0.x += y0.re;
-      t0.y += y0.im;
-      t1.x += y1.re;
-      t1.y += y1.im;
-      b0[p] = t0;
-      b1[p] = t1;
     }
-    __syncwarp();
+    A[m.A0 + p] = make_double2(s0r, s0i);
+    A[m.A1 + p] = make_double2(s1r, s1i);
   }
-  if (in_smem) {
-    for (int i = lane; i < L; i += 32) {
-      A[s0 + i] = b0[i];
-      A[s1 + i] = b1[i];
+}
+
+// packed layout (the assembly path): per contribution the two value indices
+// come straight from the plan
+template <typename R>
+__global__ void __launch_bounds__(PG_WARPS * 32)
+    k_gather_packed(const int32_t *ent_ptr, const int2 *pidx, const uint16_t *posoff, int64_t E, int64_t F,
+                    int64_t n_values, const int32_t *indptr, const void *v, double ar, double ai, double2 *A) {
+  const int lane = threadIdx.x & 31;
+  ChunkMeta m;
+  if (!chunk_meta(ent_ptr, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
+  const int total = 20 * (m.I1 - m.I0);
+  const int2 *plist = pidx + (int64_t)20 * m.I0;
+  for (int p = lane; p < m.Lsum; p += 32) {
+    const int o0 = posoff[m.hbase + p];
+    const int o1 = min(p + 1 < m.Lsum ? (int)posoff[m.hbase + p + 1] : total, total);
+    double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
+    for (int k = o0; k < o1; ++k) {
+      const int2 q = __ldg(plist + k);
+      if ((uint32_t)q.x >= (uint64_t)n_values || (uint32_t)q.y >= (uint64_t)n_values) continue;
+      const C64 u0 = load_val<R>(v, q.x), u1 = load_val<R>(v, q.y);
+      s0r += u0.re;
+      s0i += u0.im;
+      s1r += u1.re;
+      s1i += u1.im;
     }
+    A[m.A0 + p] = make_double2(ar * s0r - ai * s0i, ar * s0i + ai * s0r);
+    A[m.A1 + p] = make_double2(ar * s1r - ai * s1i, ar * s1i + ai * s1r);
   }
 }
 
@@ -125,26 +189,43 @@ __global__ void k_form_sweep(const double2 *K, const double2 *M, const double2 *
 }  // namespace
 
 int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_v1, const void *d_v2,
-                  int precision, double ar, double ai, double br, double bi, void *d_A, int64_t *d_status,
+                  int precision, int layout, double ar, double ai, double br, double bi, void *d_A, int64_t *d_status,
                   cudaStream_t s) {
+  (void)d_status;
   if (p->n_ent == 0) return EMG_OK;
+  if (precision < EMG_FP64 || precision > EMG_EXACT) return fail(EMG_EINVAL, "bad precision %d", precision);
+  if (layout != EMG_LAYOUT_COO && layout != EMG_LAYOUT_PACKED) return fail(EMG_EINVAL, "bad layout %d", layout);
   const char *plan = static_cast<const char *>(d_plan);
   const int32_t *ent_ptr = reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr);
   const Item *items = reinterpret_cast<const Item *>(plan + p->off_item);
-  const uint32_t *ent_cnt = reinterpret_cast<const uint32_t *>(plan + p->off_ent_cnt);
-  const int g = grid_for(p->n_ent, GATHER_WARPS);
+  const uint16_t *contrib = reinterpret_cast<const uint16_t *>(plan + p->off_contrib);
+  const uint16_t *posoff = reinterpret_cast<const uint16_t *>(plan + p->off_posoff);
+  const int g = grid_for(n_chunks(p->n_edges, p->n_tris), PG_WARPS);
   double2 *A = static_cast<double2 *>(d_A);
-#define EMG_GATHER(R, TWO)                                                                                         \
-  k_gather<R, TWO><<<g, GATHER_WARPS * 32, 0, s>>>(ent_ptr, items, ent_cnt, p->n_ent, p->n_edges, p->n_tris,      \
-                                                   d_indptr, d_v1, d_v2, ar, ai, br, bi, A, d_status)
-  if (precision < EMG_FP64 || precision > EMG_EXACT) return fail(EMG_EINVAL, "bad precision %d", precision);
-  if (!values_fp32(precision)) {
-    if (d_v2) EMG_GATHER(double, true); else EMG_GATHER(double, false);
-  } else {
-    if (d_v2) EMG_GATHER(float, true); else EMG_GATHER(float, false);
+  const bool two = d_v2 != nullptr;
+  const bool f32 = values_fp32(precision);
+  if (layout == EMG_LAYOUT_PACKED) {
+    if (two) return fail(EMG_EINVAL, "the packed layout takes one value array");
+    const int2 *pidx = reinterpret_cast<const int2 *>(plan + p->off_pidx);
+    const int64_t nv = p->n_assy * 210;
+    if (f32)
+      k_gather_packed<float><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, pidx, posoff, p->n_edges, p->n_tris, nv, d_indptr,
+                                                         d_v1, ar, ai, A);
+    else
+      k_gather_packed<double><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, pidx, posoff, p->n_edges, p->n_tris, nv, d_indptr,
+                                                          d_v1, ar, ai, A);
+    return launch_check("k_gather_packed");
   }
-#undef EMG_GATHER
-  return launch_check("k_gather");
+#define EMG_COO(R, TWO)                                                                                           \
+  k_gather_coo<R, TWO><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, items, contrib, posoff, p->n_edges, p->n_tris, d_indptr, \
+                                                   d_v1, d_v2, ar, ai, br, bi, A)
+  if (f32) {
+    if (two) EMG_COO(float, true); else EMG_COO(float, false);
+  } else {
+    if (two) EMG_COO(double, true); else EMG_COO(double, false);
+  }
+#undef EMG_COO
+  return launch_check("k_gather_coo");
 }
 
 int launch_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,

@@ -13,8 +13,8 @@ namespace emg {
 namespace {
 
 // 96 MiB of element-value scratch, held by every GPU that loads the library
-// until the process exits: 15,728 assembled tets in FP64/exact form (6400 B
-// per tet), 31,457 in the mixed form (3200 B per tet).
+// until the process exits: 29,959 assembled tets in FP64/exact form (3360 B
+// of packed element values per tet), 59,918 in the mixed form (1680 B).
 constexpr size_t kStaticValuesBytes = size_t(96) << 20;
 static __device__ __align__(256) unsigned char g_static_values[kStaticValuesBytes];
 

@@ -142,8 +142,9 @@ __global__ void k_count_incidence(const int32_t *t2e, const int32_t *t2t, const 
   atomicAdd(&cnt[s < 6 ? raw : E + raw], 1);
 }
 
-__global__ void k_fill_items(const int32_t *t2e, const int32_t *t2t, const int32_t *tetids, int64_t nT, int64_t nA,
-                             int64_t E, int64_t F, const int32_t *ent_ptr, int32_t *cursor, Item *items) {
+__global__ void k_fill_items(const int32_t *tets, const int32_t *t2e, const int32_t *t2t, const int32_t *tetids,
+                             int64_t nT, int64_t nA, int64_t E, int64_t F, const int32_t *ent_ptr, int32_t *cursor,
+                             Item *items) {
   int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= nA * 10) return;
   int64_t ia = g / 10;
@@ -159,7 +160,19 @@ __global__ void k_fill_items(const int32_t *t2e, const int32_t *t2t, const int32
   rec.slot = (uint8_t)s;
 #pragma unroll
   for (int k = 0; k < 10; ++k) rec.pos[k] = 0;
-  rec.pad = 0;
+  // vertex ranks by global id (a repeated vertex is caught by the element kernel)
+  int32_t v[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = tets[(int64_t)q * nT + it];
+  uint32_t ranks = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int r = 0;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) r += (v[o] < v[q] || (v[o] == v[q] && o < q)) ? 1 : 0;
+    ranks |= (uint32_t)r << (2 * q);
+  }
+  rec.ranks = (uint8_t)ranks;
   items[p] = rec;
 }
 
@@ -292,6 +305,93 @@ __global__ void k_max_col(const int32_t *col_len, int64_t n, int32_t *out) {
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// Gather lists, warp per chunk: every (item, row) of the chunk contributes to
+// one position of the chunk's first-DoF run (and the same position of its
+// second-DoF run). Count per position, scan, then place the contributions in
+// item order (items of an entity are sorted by tet), so each output sums its
+// contributions in a fixed order.
+constexpr int CC_WARPS = 8;
+
+__global__ void __launch_bounds__(CC_WARPS * 32)
+    k_chunk_contrib(const int32_t *ent_ptr, const Item *items, const uint32_t *ent_cnt, int64_t E, int64_t F,
+                    const int32_t *indptr, uint16_t *contrib, uint16_t *posoff, int2 *pidx, int64_t *st) {
+  __shared__ int32_t cnt_all[CC_WARPS][CHUNK_MAX_POS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t chunk = (int64_t)blockIdx.x * CC_WARPS + w;
+  const int64_t nec = n_edge_chunks(E);
+  if (chunk >= n_chunks(E, F)) return;
+  const bool edges = chunk < nec;
+  const int64_t x0 = edges ? chunk * CHUNK : E + (chunk - nec) * CHUNK;
+  const int nx = (int)min((int64_t)CHUNK, (edges ? E : E + F) - x0);
+  const int64_t cb0 = edges ? x0 : E + x0;
+  const int32_t my_ptr = lane <= nx ? ent_ptr[x0 + lane] : 0;
+  const int32_t my_c0 = lane <= nx ? indptr[cb0 + lane] : 0;
+  const uint32_t my_cnt = lane < nx ? ent_cnt[x0 + lane] : 0u;
+  const int32_t I0 = __shfl_sync(0xffffffffu, my_ptr, 0), I1 = __shfl_sync(0xffffffffu, my_ptr, nx);
+  const int32_t A0 = __shfl_sync(0xffffffffu, my_c0, 0), A0e = __shfl_sync(0xffffffffu, my_c0, nx);
+  const int Lsum = A0e - A0;
+  if (Lsum > CHUNK_MAX_POS || I1 - I0 > CHUNK_MAX_ITEMS) {
+    if (lane == 0) flag(st, EMG_ST_CAPACITY, x0);
+    return;
+  }
+  const int64_t hbase = edges ? (int64_t)A0 : (int64_t)indptr[E] + (A0 - indptr[2 * E]);
+  int32_t *cnt = cnt_all[w];
+  for (int i = lane; i < Lsum; i += 32) cnt[i] = 0;
+  const int r = lane;
+  const int sl = r < 6 ? r : (r < 12 ? r - 6 : (r < 16 ? r - 6 : r - 10));
+  const int blk = r < 6 ? 0 : (r < 12 ? 1 : (r < 16 ? 2 : 3));
+  __syncwarp();
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      // exclusive scan of the counts into start offsets (lane-serial blocks of 32)
+      int32_t carry = 0;
+      for (int b0 = 0; b0 < Lsum; b0 += 32) {
+        const int i = b0 + lane;
+        const int32_t v = i < Lsum ? cnt[i] : 0;
+        int32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        if (i < Lsum) {
+          cnt[i] = carry + x - v;  // becomes the cursor
+          posoff[hbase + i] = (uint16_t)(carry + x - v);
+        }
+        carry += __shfl_sync(0xffffffffu, x, 31);
+      }
+      __syncwarp();
+    }
+    for (int32_t k = I0; k < I1; ++k) {
+      if (r < 20) {
+        int e = 0;
+        for (int q = 1; q < nx; ++q)
+          if (k >= __shfl_sync(0x000fffffu, my_ptr, q)) e = q;
+        const int32_t ce = __shfl_sync(0x000fffffu, my_c0, e);
+        const uint32_t c = __shfl_sync(0x000fffffu, my_cnt, e);
+        const int ne = (int)(c & 0xffffu), nf = (int)(c >> 16);
+        const int off = blk == 0 ? 0 : (blk == 1 ? ne : (blk == 2 ? 2 * ne : 2 * ne + nf));
+        const Item rec = items[k];
+        const int p = (ce - A0) + off + rec.pos[sl];
+        if (pass == 0) {
+          cnt[p] += 1;  // distinct p across the 20 lanes of one item
+        } else {
+          const int32_t at = cnt[p]++;
+          contrib[(int64_t)20 * I0 + at] = (uint16_t)(((k - I0) << 5) | r);
+          const int s = rec.slot;
+          const int a0 = s < 6 ? s : 12 + (s - 6), a1 = s < 6 ? s + 6 : 16 + (s - 6);
+          const int al = canon_dof(rec.ranks, r);
+          const int b0 = canon_dof(rec.ranks, a0), b1 = canon_dof(rec.ranks, a1);
+          const int64_t base = (int64_t)rec.ia * 210;
+          pidx[(int64_t)20 * I0 + at] = make_int2((int)(base + packed_index(min(al, b0), max(al, b0))),
+                                                  (int)(base + packed_index(min(al, b1), max(al, b1))));
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
 }  // namespace
 
 int status_reset(int64_t *st, cudaStream_t s) {
@@ -308,6 +408,18 @@ size_t plan_layout(emg_plan *p) {
   p->off_item_pos = p->off_item;  // positions live inside the item records
   p->off_ent_cnt = o;
   o = align_up(o + (size_t)p->n_ent * 4, 256);
+  // 20 contributions (uint16: item-in-chunk << 5 | row) per item, and one
+  // uint16 start offset per first-DoF output position; a column of entity x
+  // has 2 (n_adj_edges + n_adj_faces) <= 20 * items(x) entries, so 20 per item
+  // bounds the positions before nnz is known
+  p->off_contrib = o;
+  o = align_up(o + (size_t)p->n_items * 20 * 2, 256);
+  p->off_posoff = o;
+  o = align_up(o + (size_t)p->n_items * 20 * 2, 256);
+  // per contribution the packed-layout indices of its two values (first- and
+  // second-DoF column), in the same order as contrib
+  p->off_pidx = o;
+  o = align_up(o + (size_t)p->n_items * 20 * 8, 256);
   p->plan_bytes = o;
   return o;
 }
@@ -322,8 +434,9 @@ size_t plan_workspace_bytes(const emg_plan *p) {
   return w;
 }
 
-int plan_build(emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids, void *d_plan,
-               void *d_ws, int32_t *d_indptr, int64_t *d_status, cudaStream_t s) {
+int plan_build(emg_plan *p, const int32_t *d_tets, const int32_t *d_t2e, const int32_t *d_t2t,
+               const int32_t *d_tetids, void *d_plan, void *d_ws, int32_t *d_indptr, int64_t *d_status,
+               cudaStream_t s) {
   char *plan = static_cast<char *>(d_plan);
   char *ws = static_cast<char *>(d_ws);
   int32_t *ent_ptr = reinterpret_cast<int32_t *>(plan + p->off_ent_ptr);
@@ -350,8 +463,8 @@ int plan_build(emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const in
   if ((rc = exclusive_scan(cnt, p->n_ent, ent_ptr, bsum, d_status, s))) return rc;
   if (p->n_ent > 0) CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)p->n_ent * 4, s));
   if (nI > 0) {
-    k_fill_items<<<grid_for(nI, 256), 256, 0, s>>>(d_t2e, d_t2t, d_tetids, p->n_tets, p->n_assy, p->n_edges,
-                                                    p->n_tris, ent_ptr, cnt, items);
+    k_fill_items<<<grid_for(nI, 256), 256, 0, s>>>(d_tets, d_t2e, d_t2t, d_tetids, p->n_tets, p->n_assy,
+                                                    p->n_edges, p->n_tris, ent_ptr, cnt, items);
     if ((rc = launch_check("k_fill_items"))) return rc;
   }
   CUDA_TRY(cudaMemsetAsync(col_len, 0, (size_t)(p->N + 1) * 4, s));
@@ -389,7 +502,14 @@ int plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, c
   k_entity_rows<true><<<grid_for(p->n_ent, ROWS_WARPS), ROWS_WARPS * 32, 0, s>>>(
       d_t2e, d_t2t, d_tetids, p->n_tets, p->n_edges, p->n_tris, ent_ptr, items, p->n_ent, nullptr, ent_cnt,
       d_indptr, d_indices, d_status);
-  return launch_check("k_entity_rows<fill>");
+  int rc = launch_check("k_entity_rows<fill>");
+  if (rc) return rc;
+  uint16_t *contrib = reinterpret_cast<uint16_t *>(plan + p->off_contrib);
+  uint16_t *posoff = reinterpret_cast<uint16_t *>(plan + p->off_posoff);
+  int2 *pidx = reinterpret_cast<int2 *>(plan + p->off_pidx);
+  k_chunk_contrib<<<grid_for(n_chunks(p->n_edges, p->n_tris), CC_WARPS), CC_WARPS * 32, 0, s>>>(
+      ent_ptr, items, ent_cnt, p->n_edges, p->n_tris, d_indptr, contrib, posoff, pidx, d_status);
+  return launch_check("k_chunk_contrib");
 }
 
 }  // namespace emg

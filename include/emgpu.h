@@ -83,6 +83,16 @@ enum {
   EMG_OUT_M = 2,       /* mass      (the reference's "dataB") */
 };
 
+/* element-value layouts */
+enum {
+  EMG_LAYOUT_COO = 0,    /* the reference's COO block: value[ia*400 + 20*a + b], a, b
+                            reference DoF slots (curlcurl.py:449-455); symmetric */
+  EMG_LAYOUT_PACKED = 1, /* upper triangle in the canonical (vertex-rank) DoF frame:
+                            value[ia*210 + x*(41-x)/2 + (y-x)], x <= y; the
+                            assembly path's layout (each unique entry computed
+                            once, half the bytes) */
+};
+
 typedef struct {
   int kind;          /* EMG_MAT_* */
   const void *d_er;  /* complex128, layout of `kind`, required */
@@ -102,6 +112,9 @@ typedef struct {
   int64_t nnz;       /* set by emg_plan_build */
   int64_t max_col;   /* longest column, set by emg_plan_build */
   size_t off_ent_ptr, off_item, off_item_pos, off_ent_cnt; /* byte offsets in the blob */
+  size_t off_contrib, off_posoff, off_pidx; /* gather lists: per output position of
+                                     every entity chunk, its contributions as
+                                     (item, row) and as packed value indices */
   size_t plan_bytes;      /* blob size */
   size_t workspace_bytes; /* scratch needed by emg_plan_build (and only it) */
 } emg_plan;
@@ -125,36 +138,40 @@ int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tri
  * (int32) on the device, then synchronises `stream` and stores nnz/max_col in
  * *plan. Replaces precompute_csc_pattern phases 1-3 (csc_cast.py:65-126) for
  * the structured Nedelec-2 pattern (rows of column c = DoFs of every entity
- * sharing a tet with c's entity). d_tetids: int32[n_assy] or NULL (all tets). */
-int emg_plan_build(emg_plan *plan, const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri,
+ * sharing a tet with c's entity). d_tets: int32[4][n_tets] (vertex ranks of
+ * each tet go into the plan); d_tetids: int32[n_assy] or NULL (all tets). */
+int emg_plan_build(emg_plan *plan, const int32_t *d_tets, const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri,
                    const int32_t *d_tetids, void *d_plan, void *d_workspace, int32_t *d_indptr, int64_t *d_status,
                    emg_stream_t stream);
 
-/* Writes indices[nnz] (int32, sorted within each column) and the per-slot
- * column positions. Replaces precompute_csc_pattern phase 4 (csc_cast.py:131-160). */
+/* Writes indices[nnz] (int32, sorted within each column), the per-slot column
+ * positions and the gather lists (for each output position, its contributing
+ * element slots in a fixed order). Replaces precompute_csc_pattern phase 4
+ * (csc_cast.py:131-160). */
 int emg_plan_finish(const emg_plan *plan, const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri,
                     const int32_t *d_tetids, void *d_plan, const int32_t *d_indptr, int32_t *d_indices,
                     int64_t *d_status, emg_stream_t stream);
 
-/* Element kernel: per assembled tet ia the 20x20 element block in the
- * reference's COO layout, value[ia*400 + 20*a + b] for reference DoF slots
- * a, b (curlcurl.py:449-455). out = EMG_OUT_K gives the reference's dataE,
+/* Element kernel: per assembled tet ia the 20x20 element block in `layout`
+ * (EMG_LAYOUT_COO is the reference's dataE/dataB layout, 400 values per tet;
+ * EMG_LAYOUT_PACKED 210). out = EMG_OUT_K gives the reference's dataE,
  * EMG_OUT_M its dataB, EMG_OUT_LINCOMB alpha*K_e + beta*M_e. d_values is
  * complex64 for EMG_MIXED and complex128 otherwise. Replaces
  * _matrix_builder (curlcurl.py:387-456) + ned2_tet_stiff_mass (:285-380). */
 int emg_element_values(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
                        const int32_t *d_tetids, int64_t n_assy, const emg_material *mat, int precision, int out,
-                       double alpha_re, double alpha_im, double beta_re, double beta_im, void *d_values,
-                       int64_t *d_status, emg_stream_t stream);
+                       int layout, double alpha_re, double alpha_im, double beta_re, double beta_im,
+                       void *d_values, int64_t *d_status, emg_stream_t stream);
 
 /* Column gather + segmented sum: A[nnz] (complex128, CSC order of the plan)
  * = sum over element slots of alpha*V1 + beta*V2, where V1 (required) and V2
  * (optional, NULL) are element-value arrays written by emg_element_values with
- * the same precision (complex64 for EMG_MIXED, complex128 otherwise). Deterministic (fixed summation order), no atomics.
+ * the same precision (complex64 for EMG_MIXED, complex128 otherwise) and
+ * layout (EMG_LAYOUT_PACKED: V2 must be NULL). Deterministic (fixed summation order), no atomics.
  * Replaces CSCMapping.to_csc / scatter_to_csc_c16 (csc_cast.py:55-63, 162-177). */
 int emg_gather(const emg_plan *plan, const void *d_plan, const int32_t *d_indptr, const void *d_v1,
-               const void *d_v2, int precision, double alpha_re, double alpha_im, double beta_re, double beta_im,
-               void *d_A, int64_t *d_status, emg_stream_t stream);
+               const void *d_v2, int precision, int layout, double alpha_re, double alpha_im, double beta_re,
+               double beta_im, void *d_A, int64_t *d_status, emg_stream_t stream);
 
 /* Bytes of element-value scratch that emg_assemble needs. */
 size_t emg_assemble_workspace_size(int64_t n_assy, int precision);
@@ -174,7 +191,7 @@ int emg_assemble(const emg_plan *plan, const void *d_plan, const int32_t *d_indp
  * call cudaMalloc/cudaFree, which synchronise the device). It has no
  * counterpart in the reference. The element-value scratch is a file-scope
  * device array of 96 MiB that every GPU loading this library holds until
- * exit: at most 15,728 assembled tets in EMG_FP64/EMG_EXACT, 31,457 in
+ * exit: at most 29,959 assembled tets in EMG_FP64/EMG_EXACT, 59,918 in
  * EMG_MIXED; larger plans return EMG_ERANGE. It calls no cudaMalloc/cudaFree.
  * The first call on a device looks the array's address up on that device
  * (cudaGetSymbolAddress); make that first call before any stream capture.
