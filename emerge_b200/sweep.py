@@ -1,0 +1,70 @@
+"""Frequency sweep on a resident mesh (the cached multi-frequency path of
+assembler.py:455-494).
+
+The reference caches the COO arrays Evec (K) and Bvec (M) when no material is
+frequency dependent and, per frequency, runs ``to_csc(Evec - Bvec * k0**2)``.
+Here K and M are gathered once into CSC values that stay in HBM, and
+``emg_form_sweep`` forms A_f = a_f*K + b_f*M (+ c_f*P) for a batch of
+frequencies, reading K, M (and P) once per batch.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+from scipy.sparse import csc_matrix
+
+from . import _lib as L
+from .assembly import ElemValues, GpuCSCMapping
+
+C0 = 299792458.0
+
+
+class FrequencySweep:
+    """K and M of one assembly resident on the device; A(f) on demand."""
+
+    def __init__(self, E: ElemValues, B: ElemValues, cscmap: GpuCSCMapping, P: torch.Tensor | None = None):
+        if E.job is not B.job:
+            raise ValueError("E and B must come from the same tet_mass_stiffness_matrices call")
+        self.cscmap = cscmap
+        self.K = cscmap.to_device(E)
+        self.M = cscmap.to_device(B)
+        self.P = P
+        if P is not None and (P.dtype != torch.complex128 or P.numel() != cscmap.nnz):
+            raise ValueError("P must be complex128 values in the mapping's CSC order")
+        self.nnz = cscmap.nnz
+
+    @staticmethod
+    def coefficients(freqs, gamma=None) -> np.ndarray:
+        """(nf, 6) coefficients (a, b, c) of A_f = K - k0^2 M + gamma_f P."""
+        f = np.atleast_1d(np.asarray(freqs, dtype=np.float64))
+        k0 = 2 * np.pi * f / C0
+        c = np.zeros((f.size, 6))
+        c[:, 0] = 1.0
+        c[:, 2] = -(k0 ** 2)
+        if gamma is not None:
+            g = np.broadcast_to(np.asarray(gamma, dtype=np.complex128), f.shape)
+            c[:, 4], c[:, 5] = g.real, g.imag
+        return c
+
+    def form(self, coef: np.ndarray, out: torch.Tensor | None = None) -> torch.Tensor:
+        """A values for each row of ``coef`` (nf x 6), into out[nf, nnz]
+        (complex128, device); stream-ordered."""
+        coef = np.ascontiguousarray(coef, dtype=np.float64)
+        nf = coef.shape[0]
+        if out is None:
+            out = torch.empty((nf, self.nnz), dtype=torch.complex128, device=self.K.device)
+        if out.shape != (nf, self.nnz) or not out.is_contiguous():
+            raise ValueError("out must be a contiguous (nf, nnz) complex128 tensor")
+        L.check(L.lib().emg_form_sweep(L.ptr(self.K), L.ptr(self.M), L.ptr(self.P), self.nnz,
+                                       coef.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nf, L.ptr(out), self.nnz,
+                                       L.stream_handle(self.K.device)))
+        return out
+
+    def to_csc(self, freq: float, gamma=None) -> csc_matrix:
+        a = self.form(self.coefficients([freq], gamma))[0]
+        host = torch.empty(a.shape, dtype=torch.complex128, pin_memory=True)
+        host.copy_(a)
+        m = self.cscmap
+        return csc_matrix((host.numpy(), m.indices, m.indptr), shape=(m.N, m.N))

@@ -85,3 +85,71 @@ def alg_bytes(n_nodes: int, n_tets: int, nnz: int, material_bytes_per_tet: int =
 def floor_bytes(n_nodes: int, n_tets: int, nnz: int, material_bytes_per_tet: int = 16) -> int:
     """Compulsory traffic without the mandated map: inputs + A written."""
     return 24 * n_nodes + 16 * n_tets + material_bytes_per_tet * n_tets + 16 * nnz
+
+
+def wr90_pml_slivers(n=(84, 50, 40), jitter=0.05, seed=4, freq=10e9, shell=0.10, sliver_frac=0.02,
+                     sliver_aspect=50.0) -> Workload:
+    """1,008,000-tet box (84x50x40 hexes over the WR-90 footprint) whose outer
+    10% shell carries a diagonal complex uniaxial PML tensor, with 2% of the
+    tets turned into slivers.
+
+    PML: per axis s_a = 1 - j * sigma_a / k0 with sigma_a = sigma_max * (d_a /
+    delta)^2, d_a the depth into the shell along axis a, delta the shell
+    thickness along that axis and sigma_max = 2 / delta (so sigma / k0 is
+    dimensionless); er = ur = diag(s_y s_z / s_x, s_z s_x / s_y, s_x s_y / s_z)
+    (the stretched-coordinate form of geo/pmlbox.py:80-92).
+
+    Slivers: for a seeded 2% of tets one vertex is moved toward the plane of
+    its opposite face until its height is 1/50 of the face's circumradius-scale
+    edge length; tets that any move inverts are re-oriented (det > 0 kept in
+    FP64 for every tet)."""
+    from .mesh import orient_positive, tet_signed_volumes
+
+    size = WR90
+    nodes, tets = structured_box(*n, size=size, jitter=jitter, seed=seed)
+    rng = np.random.default_rng(seed + 77)
+    nT = tets.shape[1]
+    pick = np.sort(rng.choice(nT, int(round(sliver_frac * nT)), replace=False))
+    nodes = nodes.copy()
+    used = np.zeros(nodes.shape[1], bool)
+    for t in pick:
+        q = int(rng.integers(0, 4))
+        v = tets[q, t]
+        if used[v]:
+            continue
+        others = [tets[k, t] for k in range(4) if k != q]
+        a, b, c = (nodes[:, o] for o in others)
+        nrm = np.cross(b - a, c - a)
+        nn = np.linalg.norm(nrm)
+        if nn == 0:
+            continue
+        nrm /= nn
+        h = float(np.dot(nodes[:, v] - a, nrm))
+        edge = max(np.linalg.norm(b - a), np.linalg.norm(c - a), np.linalg.norm(c - b))
+        target = np.sign(h) * edge / sliver_aspect
+        nodes[:, v] = nodes[:, v] - (h - target) * nrm
+        used[v] = True
+    tets = orient_positive(nodes, tets)
+    vol = tet_signed_volumes(nodes, tets)
+    if not (vol > 0).all():
+        raise RuntimeError("sliver construction produced a zero-volume tet")
+    f = Nedelec2Field(TetMesh(nodes, tets))
+    # PML tensors from tet centroids
+    cen = nodes[:, tets].mean(axis=1)  # (3, nT)
+    k0 = 2 * np.pi * freq / C0
+    s = np.ones((3, nT), np.complex128)
+    for ax in range(3):
+        L = size[ax]
+        delta = shell * L
+        smax = 2.0 / delta
+        d = np.maximum(np.maximum(delta - cen[ax], cen[ax] - (L - delta)), 0.0)
+        s[ax] = 1.0 - 1j * smax * (d / delta) ** 2 / k0
+    diag = np.stack([s[1] * s[2] / s[0], s[2] * s[0] / s[1], s[0] * s[1] / s[2]])
+    er = np.zeros((3, 3, nT), np.complex128)
+    ur = np.zeros((3, 3, nT), np.complex128)
+    for a in range(3):
+        er[a, a] = diag[a]
+        ur[a, a] = diag[a]
+    wl = Workload("wr90_pml_slivers", f, er, ur, np.zeros(0, np.int64), freq, tuple(n))
+    wl.slivers = pick
+    return wl
