@@ -43,6 +43,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="hex grid nx,ny,nz of the dielectric box (default 100,50,67)")
     ap.add_argument("--forms", default="fp64,mixed", help="comma list of forms to time (fp64, mixed, exact)")
+    ap.add_argument("--shard", action="store_true",
+                    help="strong scaling: one assembly column-sharded over the ranks instead of one replica per rank")
+    ap.add_argument("--serving", action="store_true",
+                    help="serving stream instead: Poisson arrivals of assembly jobs (5k-500k tets, 1-64 frequencies)")
+    ap.add_argument("--serving-jobs", type=int, default=50)
+    ap.add_argument("--serving-rate", type=float, default=50.0, help="mean arrivals per second")
+    ap.add_argument("--serving-budget-gb", type=float, default=120.0)
     return ap.parse_args()
 
 
@@ -321,18 +328,27 @@ def run_ours(args, rank, world, local_rank):
         primary = "mixed" if "mixed" in results else next(iter(results))
         mx = results[primary]
         fp = results.get("fp64", mx)
-        dom = "k_element" if mx["k_element_ms"] >= mx["k_gather_ms"] else "k_gather"
-        traffic = load_traffic(wl.name)
+        traffic = load_traffic(wl.name) or {}
 
-        def roof(r):
-            ach = balg / (r["ms"] * 1e-3) / 1e9
-            return {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                    "peak_source": peak_src, "scope": "whole assembly step (k_element + k_gather), algorithmic "
-                                                      "bytes B_alg", "floor_frac": bfloor / (r["ms"] * 1e-3) / 1e9 / hbm}
+        def roof(r, form):
+            vb = 8 if form == "mixed" else 16
+            kb = {"k_element": W.element_alg_bytes(nN, nT, vb, 16), "k_gather": W.gather_alg_bytes(nT, nnz, vb)}
+            kms = {"k_element": r["k_element_ms"], "k_gather": r["k_gather_ms"]}
+            dom = max(kms, key=kms.get)
+            kern = {}
+            for k in kb:
+                ach = kb[k] / (kms[k] * 1e-3) / 1e9
+                kern[k] = {"alg_bytes": kb[k], "ms": kms[k], "achieved": ach, "frac": ach / hbm,
+                           "traffic": traffic.get(f"{form}_{k}_bytes")}
+            step_ach = balg / (r["ms"] * 1e-3) / 1e9
+            d = kern[dom]
+            return {"bound": "hbm", "kernel": dom, "achieved": d["achieved"], "peak": hbm, "unit": "GB/s",
+                    "frac": d["frac"], "traffic": d["traffic"], "peak_source": peak_src,
+                    "alg_bytes_per_launch": d["alg_bytes"], "kernels": kern,
+                    "step": {"alg_bytes": balg, "achieved": step_ach, "frac": step_ach / hbm,
+                             "floor_bytes": bfloor, "floor_frac": bfloor / (r["ms"] * 1e-3) / 1e9 / hbm,
+                             "traffic": traffic.get(f"{form}_step_bytes")}}
 
-        rf = roof(mx)
-        rf["traffic"] = (traffic or {}).get("mixed_step_bytes")
-        rf["dominant_kernel"] = dom
         value = world * nT / (mx["ms"] * 1e-3)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": mx["ms"], "higher_is_better": True, "scaling": "weak",
@@ -345,11 +361,84 @@ def run_ours(args, rank, world, local_rank):
                            "plan_build_s": plan_s},
                 "plain_fp64": {"value": world * nT / (fp["ms"] * 1e-3), "ms_per_step": fp["ms"],
                                "k_element_ms": fp["k_element_ms"], "k_gather_ms": fp["k_gather_ms"],
-                               "roofline": roof(fp)},
+                               "roofline": roof(fp, "fp64")},
                 "mixed": {"k_element_ms": mx["k_element_ms"], "k_gather_ms": mx["k_gather_ms"]},
                 "mixed_over_plain": fp["ms"] / mx["ms"],
-                "roofline": rf, "clocks": mx["clocks"], "e2e": e2e, "gpu_launches": 2 * args.steps}
+                "roofline": roof(mx, primary), "clocks": mx["clocks"], "e2e": e2e, "gpu_launches": 2 * args.steps}
     return line, wl
+
+
+def run_shard(args, rank, world, local_rank):
+    """--shard: the workload's columns split over the ranks (each rank
+    assembles the tets touching its edges/faces, no exchange step); one step
+    = every rank assembling its column block; max-over-ranks device time."""
+    import torch
+
+    from emerge_b200.partition import ShardedAssembly, shard_of
+    from emerge_b200.ranks import max_over_ranks, sum_over_ranks
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = make_workload(args.config, grid=args.grid)
+    f = wl.field
+    t0 = time.perf_counter()
+    sh = shard_of(f.mesh, rank, world, wl.conductor_tets)
+    sa = ShardedAssembly(f, wl.er, wl.ur, sh, "mixed", dev)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    alpha, beta = 1.0 + 0j, complex(-wl.k0 ** 2)
+    out = torch.empty(sa.cmap.nnz, dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        ms = time_steps(lambda: sa.assemble(alpha, beta, out), args.steps, args.warmup, stream)
+    sa.dmesh.check_status()
+    ms, setup_s = max_over_ranks([ms, setup_s], dev)
+    own, tets_done = sum_over_ranks([sa.own_nnz, sh.tetids.size], dev)
+    if rank != 0:
+        return None
+    return {"metric": METRIC, "value": f.ntets / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "mixed", "data": "synthetic",
+            "config": {"workload": wl.name, "tets": f.ntets, "hex_grid": list(wl.hex_grid),
+                       "parallelism": f"column shards x{world}", "owned_nnz_total": int(own),
+                       "tets_assembled_total": int(tets_done), "halo_overhead": tets_done / f.ntets - 1.0,
+                       "setup_s": setup_s},
+            "clocks": sampler.summary(), "gpu_launches": 2 * args.steps}
+
+
+def run_serving(args, rank, world, local_rank):
+    """Serving stream on this rank's GPU (replicas under torchrun: each rank
+    serves its own seeded stream). Throughput in tet-frequencies/s."""
+    import torch
+
+    from emerge_b200.serving import AssemblyServer, run_stream, synthetic_stream
+
+    torch.cuda.set_device(local_rank)
+    jobs, arr = synthetic_stream(args.serving_jobs, args.serving_rate, seed=rank)
+    warm, warr = synthetic_stream(3, 1000.0, tets=(5_000, 50_000), n_freq=(1, 4), seed=1000 + rank)
+    with AssemblyServer(device=local_rank, budget_bytes=args.serving_budget_gb * 1e9, precision="mixed") as srv:
+        run_stream(srv, warm, warr)
+        srv.n_batches = srv.n_items = 0
+        srv.peak_in_use = 0
+        sampler = ClockSampler(local_rank)
+        with sampler:
+            r = run_stream(srv, jobs, arr)
+    r["clocks"] = sampler.summary()
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([r["makespan_s"], r["p99_ms"]], device=torch.device("cuda", local_rank))
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        r["makespan_s"], r["p99_ms"] = float(t[0]), float(t[1])
+    line = {"metric": "serving throughput: tet-frequencies/s assembled (A(f) = K - k0(f)^2 M on the device)",
+            "value": world * r["tet_freqs"] / r["makespan_s"], "unit": "tet-freqs/s", "n_gpus": world,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mixed", "data": "synthetic",
+            "config": {"workload": "serving_stream", "jobs": r["jobs"], "rate_per_s": args.serving_rate,
+                       "tets": "log-uniform [5k, 500k]", "freqs": "U{1..64} in U[1, 40] GHz",
+                       "budget_gb": args.serving_budget_gb, "parallelism": f"replicas x{world}"},
+            "serving": r}
+    return line if rank == 0 else None
 
 
 def main():
@@ -371,8 +460,13 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    line, wl = run_ours(args, rank, world, local_rank)
-    if rank == 0 and not args.no_cpu_baseline:
+    if args.serving:
+        line, wl = run_serving(args, rank, world, local_rank), None
+    elif args.shard:
+        line, wl = run_shard(args, rank, world, local_rank), None
+    else:
+        line, wl = run_ours(args, rank, world, local_rank)
+    if rank == 0 and not args.no_cpu_baseline and wl is not None:
         line["cpu_baseline"] = CpuBaseline(wl, args.cpu_sample_tets).measure()
     if world > 1:
         import torch.distributed as dist

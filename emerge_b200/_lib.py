@@ -23,7 +23,7 @@ EMG_LAYOUT_COO, EMG_LAYOUT_PACKED = 0, 1
 EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
-    "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc",
+    "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch",
 )
 
 
@@ -48,6 +48,14 @@ class Plan(ctypes.Structure):
         ("plan_bytes", ctypes.c_size_t),
         ("workspace_bytes", ctypes.c_size_t),
     ]
+
+
+class FormItem(ctypes.Structure):
+    _fields_ = [("K", ctypes.c_void_p), ("M", ctypes.c_void_p), ("P", ctypes.c_void_p), ("out", ctypes.c_void_p),
+                ("nnz", ctypes.c_int64), ("coef", ctypes.c_double * 6)]
+
+
+FORM_TILE = 32768
 
 
 class Material(ctypes.Structure):
@@ -86,11 +94,12 @@ def lib():
     L.emg_assemble.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
                                ctypes.c_int, _D, _D, _D, _D, _P, ctypes.c_size_t, _P, _P, _P]
     L.emg_form_sweep.argtypes = [_P, _P, _P, _I64, ctypes.POINTER(_D), ctypes.c_int, _P, _I64, _P]
+    L.emg_form_batch.argtypes = [_P, _P, _P, ctypes.c_int, _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
                                        ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
     for name in ("emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
-                 "emg_assemble_noalloc"):
+                 "emg_assemble_noalloc", "emg_form_batch"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -317,10 +317,23 @@ class GpuCSCMapping:
                                     L.ptr(self.d_plan), L.ptr(self.d_indptr), L.ptr(self.d_indices),
                                     L.ptr(m.status), st))
         m.check_status()
-        self.indptr = self.d_indptr.cpu().numpy()
-        self.indices = self.d_indices[: self.nnz].cpu().numpy()
+        self._indptr = self._indices = None
         self._ws = None
         self._ws_prec = None
+
+    @property
+    def indptr(self) -> np.ndarray:
+        """Host copy of the CSC column pointers (int32 [N+1]), made on first use."""
+        if self._indptr is None:
+            self._indptr = self.d_indptr.cpu().numpy()
+        return self._indptr
+
+    @property
+    def indices(self) -> np.ndarray:
+        """Host copy of the CSC row indices (int32 [nnz]), made on first use."""
+        if self._indices is None:
+            self._indices = self.d_indices[: self.nnz].cpu().numpy()
+        return self._indices
 
     @staticmethod
     def from_field(field, conductor_tets=None, device=None) -> "GpuCSCMapping":

@@ -169,4 +169,10 @@ int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nn
   return launch_form_sweep(d_K, d_M, d_P, nnz, h_coef, nf, d_out, out_stride, S(stream));
 }
 
+int emg_form_batch(const emg_form_item *d_items, const int64_t *d_tile_start, const int32_t *d_n_items, int max_items,
+                   emg_stream_t stream) {
+  if (!d_items || !d_tile_start || !d_n_items || max_items <= 0) return fail(EMG_EINVAL, "null pointer or max_items");
+  return launch_form_batch(d_items, d_tile_start, d_n_items, max_items, S(stream));
+}
+
 }  // extern "C"

@@ -139,5 +139,7 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *indptr, 
                   cudaStream_t s);
 int launch_form_sweep(const void *K, const void *M, const void *P, int64_t nnz, const double *coef, int nf,
                       void *out, int64_t stride, cudaStream_t s);
+int launch_form_batch(const emg_form_item *items, const int64_t *tile_start, const int32_t *n_items, int max_items,
+                      cudaStream_t s);
 
 }  // namespace emg

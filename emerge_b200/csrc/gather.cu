@@ -186,6 +186,43 @@ __global__ void k_form_sweep(const double2 *K, const double2 *M, const double2 *
   }
 }
 
+// serving batch: grid-stride over tiles of all items
+constexpr int FORM_TILE = 32768;
+
+__global__ void __launch_bounds__(256) k_form_batch(const emg_form_item *items, const int64_t *tile_start,
+                                                    const int32_t *n_items_p, int max_items) {
+  const int n = min(*n_items_p, max_items);
+  if (n <= 0) return;
+  const int64_t total = tile_start[n];
+  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+    int lo = 0, hi = n - 1;  // item with tile_start[i] <= t < tile_start[i+1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tile_start[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const emg_form_item it = items[lo];
+    const int64_t b = (t - tile_start[lo]) * FORM_TILE;
+    const int64_t e = min(b + FORM_TILE, it.nnz);
+    const double2 *K = static_cast<const double2 *>(it.K);
+    const double2 *M = static_cast<const double2 *>(it.M);
+    const double2 *P = static_cast<const double2 *>(it.P);
+    double2 *out = static_cast<double2 *>(it.out);
+    const double *c = it.coef;
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      const double2 k = K[i], m = M[i];
+      double2 o;
+      o.x = c[0] * k.x - c[1] * k.y + c[2] * m.x - c[3] * m.y;
+      o.y = c[0] * k.y + c[1] * k.x + c[2] * m.y + c[3] * m.x;
+      if (P) {
+        const double2 p = P[i];
+        o.x += c[4] * p.x - c[5] * p.y;
+        o.y += c[4] * p.y + c[5] * p.x;
+      }
+      out[i] = o;
+    }
+  }
+}
+
 }  // namespace
 
 int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_v1, const void *d_v2,
@@ -226,6 +263,18 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
   }
 #undef EMG_COO
   return launch_check("k_gather_coo");
+}
+
+int launch_form_batch(const emg_form_item *items, const int64_t *tile_start, const int32_t *n_items, int max_items,
+                      cudaStream_t s) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  k_form_batch<<<sms * 4, 256, 0, s>>>(items, tile_start, n_items, max_items);
+  return launch_check("k_form_batch");
 }
 
 int launch_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,

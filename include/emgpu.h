@@ -212,6 +212,27 @@ int emg_assemble_noalloc(const emg_plan *plan, const void *d_plan, const int32_t
 int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,
                    void *d_out, int64_t out_stride, emg_stream_t stream);
 
+/* One work item of the serving batch: out[i] = a*K[i] + b*M[i] + c*P[i] for
+ * i < nnz (complex128; P may be NULL), coef = (a_re, a_im, b_re, b_im, c_re,
+ * c_im). 80 bytes. */
+typedef struct {
+  const void *K, *M, *P;
+  void *out;
+  int64_t nnz;
+  double coef[6];
+} emg_form_item;
+
+/* Persistent-grid form of a batch of (job, frequency) items that may belong
+ * to different meshes: the items are split into tiles of 32768 nonzeros and
+ * one launch of (SM count x 4) CTAs walks all tiles. The item count and the
+ * tile offsets are read from DEVICE memory (*d_n_items, d_tile_start[n+1]),
+ * so one captured CUDA graph (a host-to-device copy of a new batch followed
+ * by this launch) can be replayed for every batch. Serving-engine entry
+ * point; its per-item arithmetic is the cached sweep's to_csc(Evec - Bvec*k0**2)
+ * (assembler.py:472-494). */
+int emg_form_batch(const emg_form_item *d_items, const int64_t *d_tile_start, const int32_t *d_n_items, int max_items,
+                   emg_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
