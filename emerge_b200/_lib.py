@@ -23,7 +23,7 @@ EMG_LAYOUT_COO, EMG_LAYOUT_PACKED = 0, 1
 EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
-    "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch",
+    "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
 )
 
 
@@ -45,6 +45,7 @@ class Plan(ctypes.Structure):
         ("nnz", ctypes.c_int64), ("max_col", ctypes.c_int64), ("off_ent_ptr", ctypes.c_size_t),
         ("off_item", ctypes.c_size_t), ("off_item_pos", ctypes.c_size_t), ("off_ent_cnt", ctypes.c_size_t),
         ("off_contrib", ctypes.c_size_t), ("off_posoff", ctypes.c_size_t), ("off_pidx", ctypes.c_size_t),
+        ("off_order", ctypes.c_size_t),
         ("plan_bytes", ctypes.c_size_t),
         ("workspace_bytes", ctypes.c_size_t),
     ]
@@ -95,11 +96,12 @@ def lib():
                                ctypes.c_int, _D, _D, _D, _D, _P, ctypes.c_size_t, _P, _P, _P]
     L.emg_form_sweep.argtypes = [_P, _P, _P, _I64, ctypes.POINTER(_D), ctypes.c_int, _P, _I64, _P]
     L.emg_form_batch.argtypes = [_P, _P, _P, ctypes.c_int, _P]
+    L.emg_plan_order.argtypes = [ctypes.POINTER(Plan), _P, _P, _I64, _P, _P, _P, _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
                                        ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
     for name in ("emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
-                 "emg_assemble_noalloc", "emg_form_batch"):
+                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

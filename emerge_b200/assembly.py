@@ -292,7 +292,9 @@ class GpuCSCMapping:
     sparsity pattern (indptr, indices: bit-identical to the reference's) and
     the column-gather plan, built once per mesh and assembled-tet set."""
 
-    def __init__(self, dmesh: DeviceMesh):
+    def __init__(self, dmesh: DeviceMesh, chunk_order: str = "morton"):
+        if chunk_order not in ("morton", "interleave"):
+            raise ValueError(f"chunk_order must be 'morton' or 'interleave', got {chunk_order!r}")
         lib = L.lib()
         m = dmesh
         self.device = m.device
@@ -310,12 +312,15 @@ class GpuCSCMapping:
         st = L.stream_handle(m.device)
         L.check(lib.emg_plan_build(L.ctypes.byref(plan), L.ptr(m.tets), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids),
                                    L.ptr(self.d_plan), L.ptr(ws), L.ptr(self.d_indptr), L.ptr(m.status), st))
-        del ws
         self.nnz = int(plan.nnz)
         self.d_indices = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=m.device)
         L.check(lib.emg_plan_finish(L.ctypes.byref(plan), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids),
                                     L.ptr(self.d_plan), L.ptr(self.d_indptr), L.ptr(self.d_indices),
                                     L.ptr(m.status), st))
+        if chunk_order == "morton":
+            L.check(lib.emg_plan_order(L.ctypes.byref(plan), L.ptr(self.d_plan), L.ptr(m.nodes), m.n_nodes,
+                                       L.ptr(m.tets), L.ptr(m.tetids), L.ptr(ws), st))
+        del ws
         m.check_status()
         self._indptr = self._indices = None
         self._ws = None

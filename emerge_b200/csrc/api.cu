@@ -169,6 +169,15 @@ int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nn
   return launch_form_sweep(d_K, d_M, d_P, nnz, h_coef, nf, d_out, out_stride, S(stream));
 }
 
+int emg_plan_order(const emg_plan *p, void *d_plan, const double *d_nodes, int64_t n_nodes, const int32_t *d_tets,
+                   const int32_t *d_tetids, void *d_ws, emg_stream_t stream) {
+  if (!p || !d_plan || n_nodes < 0 || (p->n_assy > 0 && (!d_nodes || !d_tets || !d_ws)))
+    return fail(EMG_EINVAL, "null pointer or bad size");
+  if (p->n_assy > 0 && p->n_assy < p->n_tets && !d_tetids)
+    return fail(EMG_EINVAL, "tetids required when n_assy < n_tets");
+  return plan_order(p, d_plan, d_nodes, n_nodes, d_tets, d_tetids, d_ws, S(stream));
+}
+
 int emg_form_batch(const emg_form_item *d_items, const int64_t *d_tile_start, const int32_t *d_n_items, int max_items,
                    emg_stream_t stream) {
   if (!d_items || !d_tile_start || !d_n_items || max_items <= 0) return fail(EMG_EINVAL, "null pointer or max_items");

@@ -108,6 +108,23 @@ __host__ __device__ __forceinline__ int64_t n_chunks(int64_t E, int64_t F) {
   return n_edge_chunks(E) + (F + CHUNK - 1) / CHUNK;
 }
 
+// Default processing order g -> chunk. Edge chunks and face chunks are each
+// sorted by their entities' lowest node; interleaving them in proportion keeps
+// the edge and face chunks of one mesh region together.
+__host__ __device__ __forceinline__ int64_t chunk_at(int64_t g, int64_t nec, int64_t nch) {
+  const int64_t ce0 = (g * nec) / nch, ce1 = ((g + 1) * nec) / nch;
+  return ce1 > ce0 ? ce0 : nec + (g - ce0);
+}
+
+// CTAs of a persistent grid: per_sm per SM of the current device
+inline int persistent_ctas(int per_sm) {
+  static int sms[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148 * per_sm;
+  if (!sms[dev] && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms[dev] = 0;
+  return (sms[dev] > 0 ? sms[dev] : 148) * per_sm;
+}
+
 // element kernel launchers, one translation unit per (form, material kind);
 // form 0 = reference-faithful FP64, 1 = mixed, 2 = exact closed form
 #define EMG_DECLARE_ELEM(F, K) int launch_element_##F##_##K(const ElemArgs &a, int layout, cudaStream_t s);
@@ -131,6 +148,8 @@ int plan_build(emg_plan *p, const int32_t *tets, const int32_t *t2e, const int32
                void *d_plan, void *d_ws, int32_t *indptr, int64_t *st, cudaStream_t s);
 int plan_finish(const emg_plan *p, const int32_t *t2e, const int32_t *t2t, const int32_t *tetids, void *d_plan,
                 const int32_t *indptr, int32_t *indices, int64_t *st, cudaStream_t s);
+int plan_order(const emg_plan *p, void *d_plan, const double *nodes, int64_t nN, const int32_t *tets,
+               const int32_t *tetids, void *d_ws, cudaStream_t s);
 int status_reset(int64_t *st, cudaStream_t s);
 
 // gather.cu

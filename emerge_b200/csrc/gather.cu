@@ -49,22 +49,17 @@ struct ChunkMeta {
   int64_t hbase;
 };
 
-// Processing position g -> chunk. Edge chunks and face chunks are each sorted
-// by their entities' lowest node; interleaving them in proportion keeps the
-// edge and face chunks of one mesh region together, so the element values of
-// that region's tets are read while still in L2.
-__device__ __forceinline__ int64_t chunk_at(int64_t g, int64_t nec, int64_t nch) {
-  const int64_t ce0 = (g * nec) / nch, ce1 = ((g + 1) * nec) / nch;
-  return ce1 > ce0 ? ce0 : nec + (g - ce0);
-}
-
-__device__ __forceinline__ bool chunk_meta(const int32_t *ent_ptr, const int32_t *indptr, int64_t E, int64_t F,
-                                           int64_t g, ChunkMeta &m) {
+// Processing position g -> chunk through the plan's order array (the default
+// interleave, or a spatial order from emg_plan_order), so that the element
+// values of a region's tets are read while still in L2.
+__device__ __forceinline__ bool chunk_meta(const int32_t *ent_ptr, const int32_t *order, const int32_t *indptr,
+                                           int64_t E, int64_t F, int64_t g, ChunkMeta &m) {
   const int lane = threadIdx.x & 31;
   const int64_t nec = n_edge_chunks(E);
   const int64_t nch = n_chunks(E, F);
   if (g >= nch) return false;
-  const int64_t chunk = chunk_at(g, nec, nch);
+  const int64_t chunk = __ldg(order + g);
+  if (chunk < 0 || chunk >= nch) return false;  // only a corrupted plan can hold this
   const bool edges = chunk < nec;
   const int64_t x0 = edges ? chunk * CHUNK : E + (chunk - nec) * CHUNK;
   const int nx = (int)min((int64_t)CHUNK, (edges ? E : E + F) - x0);
@@ -91,12 +86,12 @@ __device__ __forceinline__ bool chunk_meta(const int32_t *ent_ptr, const int32_t
 // reference COO layout (any COO data of this field's slot layout)
 template <typename R, bool TWO>
 __global__ void __launch_bounds__(PG_WARPS * 32)
-    k_gather_coo(const int32_t *ent_ptr, const Item *items, const uint16_t *contrib, const uint16_t *posoff,
-                 int64_t E, int64_t F, const int32_t *indptr, const void *v1, const void *v2, double ar, double ai,
+    k_gather_coo(const int32_t *ent_ptr, const int32_t *order, const Item *items, const uint16_t *contrib,
+                 const uint16_t *posoff, int64_t E, int64_t F, const int32_t *indptr, const void *v1, const void *v2, double ar, double ai,
                  double br, double bi, double2 *A) {
   const int lane = threadIdx.x & 31;
   ChunkMeta m;
-  if (!chunk_meta(ent_ptr, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
+  if (!chunk_meta(ent_ptr, order, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
   const int total = 20 * (m.I1 - m.I0);
   const uint16_t *clist = contrib + (int64_t)20 * m.I0;
   const Item *it = items + m.I0;
@@ -133,11 +128,11 @@ __global__ void __launch_bounds__(PG_WARPS * 32)
 // come straight from the plan
 template <typename R>
 __global__ void __launch_bounds__(PG_WARPS * 32)
-    k_gather_packed(const int32_t *ent_ptr, const int2 *pidx, const uint16_t *posoff, int64_t E, int64_t F,
-                    int64_t n_values, const int32_t *indptr, const void *v, double ar, double ai, double2 *A) {
+    k_gather_packed(const int32_t *ent_ptr, const int32_t *order, const int2 *pidx, const uint16_t *posoff,
+                    int64_t E, int64_t F, int64_t n_values, const int32_t *indptr, const void *v, double ar, double ai, double2 *A) {
   const int lane = threadIdx.x & 31;
   ChunkMeta m;
-  if (!chunk_meta(ent_ptr, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
+  if (!chunk_meta(ent_ptr, order, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
   const int total = 20 * (m.I1 - m.I0);
   const int2 *plist = pidx + (int64_t)20 * m.I0;
   for (int p = lane; p < m.Lsum; p += 32) {
@@ -235,6 +230,7 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
   const char *plan = static_cast<const char *>(d_plan);
   const int32_t *ent_ptr = reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr);
   const Item *items = reinterpret_cast<const Item *>(plan + p->off_item);
+  const int32_t *order = reinterpret_cast<const int32_t *>(plan + p->off_order);
   const uint16_t *contrib = reinterpret_cast<const uint16_t *>(plan + p->off_contrib);
   const uint16_t *posoff = reinterpret_cast<const uint16_t *>(plan + p->off_posoff);
   const int g = grid_for(n_chunks(p->n_edges, p->n_tris), PG_WARPS);
@@ -246,16 +242,16 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
     const int2 *pidx = reinterpret_cast<const int2 *>(plan + p->off_pidx);
     const int64_t nv = p->n_assy * 210;
     if (f32)
-      k_gather_packed<float><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, pidx, posoff, p->n_edges, p->n_tris, nv, d_indptr,
-                                                         d_v1, ar, ai, A);
+      k_gather_packed<float><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, order, pidx, posoff, p->n_edges, p->n_tris, nv,
+                                                         d_indptr, d_v1, ar, ai, A);
     else
-      k_gather_packed<double><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, pidx, posoff, p->n_edges, p->n_tris, nv, d_indptr,
-                                                          d_v1, ar, ai, A);
+      k_gather_packed<double><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, order, pidx, posoff, p->n_edges, p->n_tris, nv,
+                                                          d_indptr, d_v1, ar, ai, A);
     return launch_check("k_gather_packed");
   }
 #define EMG_COO(R, TWO)                                                                                           \
-  k_gather_coo<R, TWO><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, items, contrib, posoff, p->n_edges, p->n_tris, d_indptr, \
-                                                   d_v1, d_v2, ar, ai, br, bi, A)
+  k_gather_coo<R, TWO><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, order, items, contrib, posoff, p->n_edges, p->n_tris, \
+                                                   d_indptr, d_v1, d_v2, ar, ai, br, bi, A)
   if (f32) {
     if (two) EMG_COO(float, true); else EMG_COO(float, false);
   } else {
@@ -267,13 +263,7 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
 
 int launch_form_batch(const emg_form_item *items, const int64_t *tile_start, const int32_t *n_items, int max_items,
                       cudaStream_t s) {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  }
-  k_form_batch<<<sms * 4, 256, 0, s>>>(items, tile_start, n_items, max_items);
+  k_form_batch<<<persistent_ctas(4), 256, 0, s>>>(items, tile_start, n_items, max_items);
   return launch_check("k_form_batch");
 }
 

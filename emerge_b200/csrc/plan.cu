@@ -392,6 +392,115 @@ __global__ void __launch_bounds__(CC_WARPS * 32)
   }
 }
 
+__global__ void k_default_order(int32_t *order, int64_t nec, int64_t nch) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < nch) order[g] = (int32_t)chunk_at(g, nec, nch);
+}
+
+// bounding box of the nodes (SoA [3][nN]): per-block partials, then one block
+__global__ void __launch_bounds__(256) k_bbox_partial(const double *nodes, int64_t nN, double *part) {
+  __shared__ double sm[6][256];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nN; i += (int64_t)gridDim.x * blockDim.x)
+    for (int d = 0; d < 3; ++d) {
+      const double x = nodes[d * nN + i];
+      lo[d] = fmin(lo[d], x);
+      hi[d] = fmax(hi[d], x);
+    }
+  for (int d = 0; d < 3; ++d) {
+    sm[d][threadIdx.x] = lo[d];
+    sm[3 + d][threadIdx.x] = hi[d];
+  }
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int d = 0; d < 3; ++d) {
+        sm[d][threadIdx.x] = fmin(sm[d][threadIdx.x], sm[d][threadIdx.x + st]);
+        sm[3 + d][threadIdx.x] = fmax(sm[3 + d][threadIdx.x], sm[3 + d][threadIdx.x + st]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) part[blockIdx.x * 6 + threadIdx.x] = sm[threadIdx.x][0];
+}
+
+__global__ void k_bbox_final(const double *part, int nblk, double *box) {
+  if (threadIdx.x < 6) {
+    double v = part[threadIdx.x];
+    for (int b = 1; b < nblk; ++b) {
+      const double x = part[b * 6 + threadIdx.x];
+      v = threadIdx.x < 3 ? fmin(v, x) : fmax(v, x);
+    }
+    box[threadIdx.x] = v;
+  }
+}
+
+__device__ __forceinline__ uint32_t spread_bits10(uint32_t x) {  // bit i -> bit 3i
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// key of chunk c = Morton code of the centroid of its first incident tet in
+// the high 32 bits, c in the low 32 bits; chunks without items and the
+// padding up to the power of two sort last
+__global__ void k_chunk_keys(const int32_t *ent_ptr, const Item *items, const double *nodes, int64_t nN,
+                             const int32_t *tets, int64_t nT, const int32_t *tetids, int64_t nA, const double *box,
+                             int64_t E, int64_t F, int64_t nch, int64_t n2, uint64_t *keys) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n2) return;
+  uint64_t key = ~0ull;
+  if (c < nch) {
+    const int64_t nec = n_edge_chunks(E);
+    const int64_t x0 = c < nec ? c * CHUNK : E + (c - nec) * CHUNK;
+    const int64_t xe = min(x0 + CHUNK, c < nec ? E : E + F);
+    const int32_t i0 = ent_ptr[x0], i1 = ent_ptr[xe];
+    uint32_t code = 0xffffffffu;
+    if (i1 > i0) {
+      const int64_t ia = items[i0].ia;
+      const int64_t t = (ia >= 0 && ia < nA) ? (tetids ? (int64_t)tetids[ia] : ia) : -1;
+      if (t >= 0 && t < nT) {
+        const double ext = fmax(fmax(box[3] - box[0], box[4] - box[1]), fmax(box[5] - box[2], 1e-300));
+        uint32_t q[3];
+        for (int d = 0; d < 3; ++d) {
+          double x = 0.0;
+          for (int k = 0; k < 4; ++k) {
+            const int64_t v = tets[k * nT + t];
+            x += (v >= 0 && v < nN) ? nodes[d * nN + v] : box[d];
+          }
+          const double u = (0.25 * x - box[d]) / ext * 1024.0;
+          q[d] = (uint32_t)fmin(fmax(u, 0.0), 1023.0);
+        }
+        code = spread_bits10(q[0]) | (spread_bits10(q[1]) << 1) | (spread_bits10(q[2]) << 2);
+      }
+    }
+    key = ((uint64_t)code << 32) | (uint64_t)c;
+  }
+  keys[c] = key;
+}
+
+// one compare-exchange step (k, j) of a bitonic sort of n2 = 2^m keys
+__global__ void k_bitonic_step(uint64_t *keys, int64_t n2, int64_t j, int64_t k) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n2) return;
+  const int64_t l = i ^ j;
+  if (l > i) {
+    const uint64_t a = keys[i], b = keys[l];
+    const bool up = (i & k) == 0;
+    if ((a > b) == up) {
+      keys[i] = b;
+      keys[l] = a;
+    }
+  }
+}
+
+__global__ void k_write_order(const uint64_t *keys, int64_t nch, int32_t *order) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < nch) order[g] = (int32_t)(keys[g] & 0xffffffffu);
+}
+
 }  // namespace
 
 int status_reset(int64_t *st, cudaStream_t s) {
@@ -420,18 +529,35 @@ size_t plan_layout(emg_plan *p) {
   // second-DoF column), in the same order as contrib
   p->off_pidx = o;
   o = align_up(o + (size_t)p->n_items * 20 * 8, 256);
+  // the gather's chunk processing order
+  p->off_order = o;
+  o = align_up(o + (size_t)n_chunks(p->n_edges, p->n_tris) * 4, 256);
   p->plan_bytes = o;
   return o;
 }
 
+// chunk-order scratch: bounding-box partials and the sort keys (power of two)
+constexpr int BBOX_BLOCKS = 296;
+static int64_t pow2_at_least(int64_t n) {
+  int64_t v = 1;
+  while (v < n) v <<= 1;
+  return v;
+}
+static size_t order_workspace_bytes(const emg_plan *p) {
+  return align_up((size_t)BBOX_BLOCKS * 6 * 8 + 64, 256) +
+         (size_t)pow2_at_least(n_chunks(p->n_edges, p->n_tris)) * 8;
+}
+
 // workspace: per-entity counters, per-column lengths, scan block sums, max
+// (plan build); bounding box and sort keys (chunk order); the larger of both
 size_t plan_workspace_bytes(const emg_plan *p) {
   size_t w = 0;
   w = align_up(w + (size_t)p->n_ent * 4, 256);
   w = align_up(w + (size_t)(p->N + 1) * 4, 256);
   w = align_up(w + scan_bsum_bytes(p->N > p->n_ent ? p->N : p->n_ent), 256);
   w = align_up(w + 16, 256);
-  return w;
+  const size_t wo = order_workspace_bytes(p);
+  return w > wo ? w : wo;
 }
 
 int plan_build(emg_plan *p, const int32_t *d_tets, const int32_t *d_t2e, const int32_t *d_t2t,
@@ -494,8 +620,15 @@ int plan_build(emg_plan *p, const int32_t *d_tets, const int32_t *d_t2e, const i
 
 int plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, const int32_t *d_tetids,
                 void *d_plan, const int32_t *d_indptr, int32_t *d_indices, int64_t *d_status, cudaStream_t s) {
-  if (p->n_ent == 0 || p->n_assy == 0) return EMG_OK;
   char *plan = static_cast<char *>(d_plan);
+  const int64_t nch = n_chunks(p->n_edges, p->n_tris);
+  if (nch > 0) {
+    k_default_order<<<grid_for(nch, 256), 256, 0, s>>>(reinterpret_cast<int32_t *>(plan + p->off_order),
+                                                        n_edge_chunks(p->n_edges), nch);
+    const int rc = launch_check("k_default_order");
+    if (rc) return rc;
+  }
+  if (p->n_ent == 0 || p->n_assy == 0) return EMG_OK;
   const int32_t *ent_ptr = reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr);
   Item *items = reinterpret_cast<Item *>(plan + p->off_item);
   uint32_t *ent_cnt = reinterpret_cast<uint32_t *>(plan + p->off_ent_cnt);
@@ -510,6 +643,34 @@ int plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, c
   k_chunk_contrib<<<grid_for(n_chunks(p->n_edges, p->n_tris), CC_WARPS), CC_WARPS * 32, 0, s>>>(
       ent_ptr, items, ent_cnt, p->n_edges, p->n_tris, d_indptr, contrib, posoff, pidx, d_status);
   return launch_check("k_chunk_contrib");
+}
+
+int plan_order(const emg_plan *p, void *d_plan, const double *nodes, int64_t nN, const int32_t *tets,
+               const int32_t *tetids, void *d_ws, cudaStream_t s) {
+  const int64_t nch = n_chunks(p->n_edges, p->n_tris);
+  if (nch == 0 || p->n_assy == 0 || nN == 0) return EMG_OK;
+  char *plan = static_cast<char *>(d_plan);
+  char *ws = static_cast<char *>(d_ws);
+  double *part = reinterpret_cast<double *>(ws);
+  double *box = part + (size_t)BBOX_BLOCKS * 6;
+  uint64_t *keys = reinterpret_cast<uint64_t *>(ws + align_up((size_t)BBOX_BLOCKS * 6 * 8 + 64, 256));
+  const int64_t n2 = pow2_at_least(nch);
+  k_bbox_partial<<<BBOX_BLOCKS, 256, 0, s>>>(nodes, nN, part);
+  int rc = launch_check("k_bbox_partial");
+  if (rc) return rc;
+  k_bbox_final<<<1, 32, 0, s>>>(part, BBOX_BLOCKS, box);
+  if ((rc = launch_check("k_bbox_final"))) return rc;
+  k_chunk_keys<<<grid_for(n2, 256), 256, 0, s>>>(
+      reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr), reinterpret_cast<const Item *>(plan + p->off_item),
+      nodes, nN, tets, p->n_tets, tetids, p->n_assy, box, p->n_edges, p->n_tris, nch, n2, keys);
+  if ((rc = launch_check("k_chunk_keys"))) return rc;
+  for (int64_t k = 2; k <= n2; k <<= 1)
+    for (int64_t j = k >> 1; j > 0; j >>= 1) {
+      k_bitonic_step<<<grid_for(n2, 256), 256, 0, s>>>(keys, n2, j, k);
+      if ((rc = launch_check("k_bitonic_step"))) return rc;
+    }
+  k_write_order<<<grid_for(nch, 256), 256, 0, s>>>(keys, nch, reinterpret_cast<int32_t *>(plan + p->off_order));
+  return launch_check("k_write_order");
 }
 
 }  // namespace emg

@@ -28,6 +28,7 @@ EDGE_SLOTS = np.array([(0, 1), (0, 2), (0, 3), (1, 2), (3, 1), (2, 3)], dtype=np
 FACE_SLOTS = np.array([(0, 1, 2), (0, 2, 3), (0, 3, 1), (1, 2, 3)], dtype=np.int64)
 # dofcodes of SECOND_MIXED_VOLAKIS: edge ids [0, 2], face ids [0, 1] (dofsets.py:39,114-115)
 VOLAKIS_DOFCODES = np.array([64] * 6 + [66] * 6 + [128] * 4 + [129] * 4, dtype=np.int64)
+VOLAKIS_DOFCODES_2D = np.array([64] * 3 + [66] * 3 + [128, 129], dtype=np.int64)
 
 
 def _unique_rows(keys: np.ndarray):
@@ -48,7 +49,7 @@ def _unique_rows(keys: np.ndarray):
 class TetMesh:
     """Mesh topology in the reference's layout (``Mesh3D``): nodes f8[3,nN],
     tets i8[4,nT], edges i8[2,E], tris i8[3,F], tet_to_edge i8[6,nT],
-    tet_to_tri i8[4,nT]."""
+    tet_to_tri i8[4,nT], tri_to_edge i8[3,F]."""
 
     nodes: np.ndarray
     tets: np.ndarray
@@ -56,6 +57,7 @@ class TetMesh:
     tris: np.ndarray = field(init=False)
     tet_to_edge: np.ndarray = field(init=False)
     tet_to_tri: np.ndarray = field(init=False)
+    tri_to_edge: np.ndarray = field(init=False)
 
     def __post_init__(self):
         self.nodes = np.ascontiguousarray(self.nodes, dtype=np.float64)
@@ -76,6 +78,13 @@ class TetMesh:
         self.tris = np.ascontiguousarray(tris.T)
         self.tet_to_edge = np.ascontiguousarray(einv.reshape(nT, 6).T)
         self.tet_to_tri = np.ascontiguousarray(finv.reshape(nT, 4).T)
+        # tri_to_edge[3, F]: edges (v0,v1), (v1,v2), (v0,v2) of each sorted tri (mesh3d.py:836-839)
+        nN = self.nodes.shape[1]
+        ekey = self.edges[0] * nN + self.edges[1]
+        tr = self.tris
+        self.tri_to_edge = np.ascontiguousarray(np.stack([
+            np.searchsorted(ekey, tr[0] * nN + tr[1]), np.searchsorted(ekey, tr[1] * nN + tr[2]),
+            np.searchsorted(ekey, tr[0] * nN + tr[2])]).astype(np.int64))
 
     @property
     def n_nodes(self) -> int:
@@ -111,6 +120,14 @@ class Nedelec2Field:
         t2f[12:16] = mesh.tet_to_tri + 2 * E
         t2f[16:20] = mesh.tet_to_tri + 2 * E + F
         self.tet_to_field = t2f
+        # triangle DoFs (nedelec2.py:69-79): 3 ne0 edges, 3 ne2 edges, nf0, nf1
+        self.dofcodes2d = VOLAKIS_DOFCODES_2D.copy()
+        tf = np.empty((8, F), dtype=np.int64)
+        tf[0:3] = mesh.tri_to_edge
+        tf[3:6] = mesh.tri_to_edge + E
+        tf[6] = np.arange(F) + 2 * E
+        tf[7] = np.arange(F) + 2 * E + F
+        self.tri_to_field = tf
 
     def get_tet_to_field(self) -> np.ndarray:
         return self.tet_to_field

@@ -115,8 +115,9 @@ typedef struct {
   size_t off_contrib, off_posoff, off_pidx; /* gather lists: per output position of
                                      every entity chunk, its contributions as
                                      (item, row) and as packed value indices */
+  size_t off_order;       /* int32 per entity chunk: the gather's processing order */
   size_t plan_bytes;      /* blob size */
-  size_t workspace_bytes; /* scratch needed by emg_plan_build (and only it) */
+  size_t workspace_bytes; /* scratch needed by emg_plan_build and emg_plan_order */
 } emg_plan;
 
 int emg_version(void);
@@ -151,6 +152,18 @@ int emg_plan_build(emg_plan *plan, const int32_t *d_tets, const int32_t *d_tet_t
 int emg_plan_finish(const emg_plan *plan, const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri,
                     const int32_t *d_tetids, void *d_plan, const int32_t *d_indptr, int32_t *d_indices,
                     int64_t *d_status, emg_stream_t stream);
+
+/* Optional, after emg_plan_finish: orders the gather's entity chunks along a
+ * Morton curve of their position (the centroid of each chunk's first incident
+ * tet, quantised to 1024 cells per axis of the mesh's bounding cube), so that
+ * chunks that share tets are gathered close together in time and the shared
+ * element values are still in L2. Changes which warp computes which column
+ * run and when, never a value. Without it the gather walks edge and face
+ * chunks in a proportional interleave of their index order. d_workspace:
+ * plan->workspace_bytes. No counterpart in the reference (a GPU memory
+ * hierarchy optimisation). */
+int emg_plan_order(const emg_plan *plan, void *d_plan, const double *d_nodes, int64_t n_nodes, const int32_t *d_tets,
+                   const int32_t *d_tetids, void *d_workspace, emg_stream_t stream);
 
 /* Element kernel: per assembled tet ia the 20x20 element block in `layout`
  * (EMG_LAYOUT_COO is the reference's dataE/dataB layout, 400 values per tet;

@@ -7,6 +7,9 @@ surface on numpy arrays:
 * ``matrix_builder``   -> curlcurl.py:387-456 ``_matrix_builder``
 * ``CSCPattern``       -> csc_cast.py:29-63   ``CSCMapping`` (from_rowcol / to_csc)
 * ``tet_mass_stiffness_matrices`` -> curlcurl.py:222-270
+* ``tri_stiff``, ``robin_entries``, ``tri_rowcol``, ``generate_csc``
+                       -> robinbc.py:316-402 (``ned2_tri_stiff``,
+                          ``compute_bc_entries``), femdata.py:52-56,75-92,104-118
 * ``topology_loops``   -> mesh3d.py:706-776 and nedelec2.py:61-79 restated as
   plain Python loops (small meshes only; checks the vectorised host topology)
 
@@ -59,6 +62,10 @@ def lib():
         L.oracle_scatter_lincomb_c16.argtypes = [_p, _p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_double, _p, _p, _p, _i64, _p, ctypes.c_int]
         L.oracle_num_threads.restype = ctypes.c_int
+        L.oracle_tri_stiff.restype = None
+        L.oracle_tri_stiff.argtypes = [_p, ctypes.c_double, ctypes.c_double, _p]
+        L.oracle_robin_entries.restype = ctypes.c_int
+        L.oracle_robin_entries.argtypes = [_p, _i64, _p, _i64, _p, _i64, ctypes.c_double, ctypes.c_double, _p]
         _lib = L
     return _lib
 
@@ -188,3 +195,51 @@ def topology_loops(tets: np.ndarray):
     for i in range(2):  # nfdof = 2 (face ids [0, 1])
         t2f[12 + 4 * i:12 + 4 * (i + 1)] = t2t + i * F + 2 * E
     return edges, tris, t2e, t2t, t2f
+
+
+# ---------------------------------------------------------------- Robin boundary term
+def tri_stiff(X: np.ndarray, gamma: complex) -> np.ndarray:
+    """``ned2_tri_stiff`` (robinbc.py:316-378): X f8[3, 3] = the triangle's
+    vertex coordinates (column v = vertex v) -> c16[8, 8]."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.empty(64, np.complex128)
+    g = complex(gamma)
+    lib().oracle_tri_stiff(_ptr(X), g.real, g.imag, _ptr(out))
+    return out.reshape(8, 8)
+
+
+def robin_entries(field, tri_ids, gamma: complex, Bmat: np.ndarray | None = None) -> np.ndarray:
+    """``assemble_robin_bc`` / ``compute_bc_entries`` (robinbc.py:381-451):
+    adds every listed tri's 8x8 block into the tri COO array Bmat c16[F*64]
+    (``empty_tri_matrix``, femdata.py:52-56) at itri*64."""
+    m = field.mesh
+    F = m.tris.shape[1]
+    if Bmat is None:
+        Bmat = np.zeros(F * 64, np.complex128)
+    nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+    tris = np.ascontiguousarray(m.tris, dtype=np.int64)
+    ids = np.ascontiguousarray(tri_ids, dtype=np.int64)
+    g = complex(gamma)
+    rc = lib().oracle_robin_entries(_ptr(nodes), nodes.shape[1], _ptr(tris), F, _ptr(ids), ids.shape[0], g.real,
+                                    g.imag, _ptr(Bmat))
+    if rc != 0:
+        raise IndexError("tri id or vertex index out of range")
+    return Bmat
+
+
+def tri_rowcol(field):
+    """``empty_tri_rowcol`` (femdata.py:75-92): per tri 64 slots,
+    rows[p + 8*ii + jj] = t2f[ii], cols[...] = t2f[jj] over ``tri_to_field``."""
+    t2f = field.tri_to_field  # (8, F)
+    F = t2f.shape[1]
+    rows = np.repeat(t2f.T[:, :, None], 8, axis=2).reshape(F * 64)
+    cols = np.repeat(t2f.T[:, None, :], 8, axis=1).reshape(F * 64)
+    return rows, cols
+
+
+def generate_csc(field, data: np.ndarray) -> csc_matrix:
+    """``generate_csc`` (femdata.py:104-118) with the tri row/col arrays:
+    the nonzero slots only, duplicates summed by scipy."""
+    rows, cols = tri_rowcol(field)
+    ids = np.argwhere(data != 0)[:, 0]
+    return csc_matrix((data[ids], (rows[ids], cols[ids])), shape=(field.n_field, field.n_field))

@@ -18,6 +18,8 @@ modules directly:
 * ``emerge._emerge.mth.csc_cast`` (``CSCMapping`` :29-63,
   ``precompute_csc_pattern`` :65-160, ``scatter_to_csc_c16`` :162-177)
 * ``emerge._emerge.mth.optimized`` (``local_mapping`` :262-296, ``matinv`` :315-357)
+* ``emerge._emerge.physics.microwave.assembly.robinbc`` (``ned2_tri_stiff``
+  :316-378, ``compute_bc_entries`` :381-402)
 """
 from __future__ import annotations
 
@@ -62,4 +64,6 @@ def load_reference(ref_root: str = DEFAULT_REF_ROOT):
     ns.csc_cast = importlib.import_module("emerge._emerge.mth.csc_cast")
     ns.optimized = importlib.import_module("emerge._emerge.mth.optimized")
     ns.ccbf = importlib.import_module("emerge._emerge.compiled.ccbf")
+    # Robin boundary term (robinbc.py); imports cleanly with the stubs above
+    ns.robinbc = importlib.import_module("emerge._emerge.physics.microwave.assembly.robinbc")
     return ns

@@ -1,0 +1,145 @@
+/* CPU ORACLE -- test infrastructure, not product code.
+ *
+ * Plain-C restatement of EMerge's Robin (third-kind) boundary term on
+ * Nedelec-2 (SECOND_MIXED_VOLAKIS) triangles, the port / absorbing-boundary
+ * matrix the microwave assembler adds into A:
+ *
+ *   ned2_tri_stiff      physics/microwave/assembly/robinbc.py:316-378
+ *   construct_local_vertices                     robinbc.py:165-183
+ *   tri_coefficients                             robinbc.py:200-221
+ *   DPTS (6-point triangle rule)                 robinbc.py:189-196
+ *   compute_bc_entries                           robinbc.py:381-402
+ *   2-D basis functions _ne0_2d, _ne2_2d, _nf0_2d, _nf1_2d
+ *                                                compiled/ccbf.py:81,107,269,284
+ *
+ * dofcodes2d of the Volakis set are [64, 64, 64, 66, 66, 66, 128, 129]
+ * (elements/dofsets.py:39,114-115): three ne0 edge functions on the local
+ * vertex pairs (0,1), (1,2), (0,2), three ne2 on the same pairs, then nf0 and
+ * nf1 on (0,1,2). The triangle matrix is
+ *   B[a][b] = gamma * A * sum_q w_q (f_a . f_b)(x_q)
+ * in the triangle's own plane (unconjugated dot product, A = area).
+ */
+#include <complex.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+typedef double complex cplx;
+
+/* robinbc.py:189-196, digit for digit: weights and barycentric rows L1..L3 */
+static const double TRI_DPTS[4][6] = {
+    {0.10995174365532200, 0.10995174365532200, 0.10995174365532200, 0.22338158967801100, 0.22338158967801100,
+     0.22338158967801100},
+    {0.81684757298045896, 0.09157621350977101, 0.09157621350977101, 0.10810301816807000, 0.44594849091596500,
+     0.44594849091596500},
+    {0.09157621350977101, 0.81684757298045896, 0.09157621350977101, 0.44594849091596500, 0.10810301816807000,
+     0.44594849091596500},
+    {0.09157621350977004, 0.09157621350977008, 0.81684757298045807, 0.44594849091596500, 0.44594849091596500,
+     0.10810301816807000},
+};
+
+static void cross3(const double a[3], const double b[3], double out[3]) {
+  out[0] = a[1] * b[2] - a[2] * b[1];
+  out[1] = a[2] * b[0] - a[0] * b[2];
+  out[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static void normalize3(double a[3]) {
+  const double n = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  a[0] /= n;
+  a[1] /= n;
+  a[2] /= n;
+}
+
+/* X[d][v]: vertex v (0..2) coordinates. out[64] row-major, gamma applied. */
+void oracle_tri_stiff(const double X[3][3], double g_re, double g_im, cplx *out) {
+  /* construct_local_vertices: origin at vertex 0, x along edge 0->1, z the normal */
+  double e1[3], e2[3], xh[3], yh[3], zh[3];
+  for (int d = 0; d < 3; ++d) {
+    e1[d] = X[d][1] - X[d][0];
+    e2[d] = X[d][2] - X[d][0];
+  }
+  cross3(e1, e2, zh);
+  normalize3(zh);
+  memcpy(xh, e1, sizeof xh);
+  normalize3(xh);
+  cross3(zh, xh, yh);
+  normalize3(yh);
+  double tx[3], ty[3];
+  for (int v = 0; v < 3; ++v) {
+    double rx = 0.0, ry = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double r = X[d][v] - X[d][0];
+      rx += xh[d] * r;
+      ry += yh[d] * r;
+    }
+    tx[v] = rx;
+    ty[v] = ry;
+  }
+  /* tri_coefficients */
+  const double x1 = tx[0], x2 = tx[1], x3 = tx[2], y1 = ty[0], y2 = ty[1], y3 = ty[2];
+  const double a[3] = {x2 * y3 - y2 * x3, x3 * y1 - y3 * x1, x1 * y2 - y1 * x2};
+  const double b[3] = {y2 - y3, y3 - y1, y1 - y2};
+  const double c[3] = {x3 - x2, x1 - x3, x2 - x1};
+  const double sA = 0.5 * (b[0] * c[1] - b[1] * c[0]);
+  double ca[3], cb[3], cc[3];
+  for (int m = 0; m < 3; ++m) {
+    ca[m] = a[m] / (2 * sA);
+    cb[m] = b[m] / (2 * sA);
+    cc[m] = c[m] / (2 * sA);
+  }
+  const double area = fabs(sA);
+  /* the 8 basis functions at the 6 points */
+  static const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
+  double f[8][2][6];
+  for (int q = 0; q < 6; ++q) {
+    const double xs = tx[0] * TRI_DPTS[1][q] + tx[1] * TRI_DPTS[2][q] + tx[2] * TRI_DPTS[3][q];
+    const double ys = ty[0] * TRI_DPTS[1][q] + ty[1] * TRI_DPTS[2][q] + ty[2] * TRI_DPTS[3][q];
+    double L[3];
+    for (int m = 0; m < 3; ++m) L[m] = ca[m] + cb[m] * xs + cc[m] * ys;
+    for (int e = 0; e < 3; ++e) {
+      const int i = EI[e], j = EJ[e];
+      /* ne0: L_i grad L_j - L_j grad L_i */
+      f[e][0][q] = L[i] * cb[j] - L[j] * cb[i];
+      f[e][1][q] = L[i] * cc[j] - L[j] * cc[i];
+      /* ne2: (L_i - L_j)(L_i grad L_j - L_j grad L_i) */
+      const double s = L[i] - L[j];
+      f[3 + e][0][q] = s * (L[i] * cb[j] - L[j] * cb[i]);
+      f[3 + e][1][q] = s * (L[i] * cc[j] - L[j] * cc[i]);
+    }
+    /* nf0: L_0 (L_1 grad L_2 - L_2 grad L_1); nf1: L_1 (L_0 grad L_2 - L_2 grad L_0) */
+    f[6][0][q] = L[0] * (L[1] * cb[2] - L[2] * cb[1]);
+    f[6][1][q] = L[0] * (L[1] * cc[2] - L[2] * cc[1]);
+    f[7][0][q] = L[1] * (L[0] * cb[2] - L[2] * cb[0]);
+    f[7][1][q] = L[1] * (L[0] * cc[2] - L[2] * cc[0]);
+  }
+  const cplx g = g_re + I * g_im;
+  for (int p = 0; p < 8; ++p)
+    for (int r = 0; r < 8; ++r) {
+      double sum = 0.0;
+      for (int q = 0; q < 6; ++q) sum += (f[p][0][q] * f[r][0][q] + f[p][1][q] * f[r][1][q]) * TRI_DPTS[0][q];
+      out[8 * p + r] = g * sum * area;
+    }
+}
+
+/* compute_bc_entries: Bmat[itri*64 .. +64] += B(itri) for every listed tri.
+ * nodes f64 [3][nN], tris i64 [3][F] (sorted vertex ids). */
+int oracle_robin_entries(const double *nodes, int64_t nN, const int64_t *tris, int64_t F, const int64_t *btris,
+                         int64_t nb, double g_re, double g_im, cplx *Bmat) {
+  for (int64_t i = 0; i < nb; ++i) {
+    const int64_t t = btris[i];
+    if (t < 0 || t >= F) return -1;
+    for (int v = 0; v < 3; ++v)
+      if (tris[v * F + t] < 0 || tris[v * F + t] >= nN) return -1;
+  }
+  for (int64_t i = 0; i < nb; ++i) {
+    const int64_t t = btris[i];
+    double X[3][3];
+    for (int d = 0; d < 3; ++d)
+      for (int v = 0; v < 3; ++v) X[d][v] = nodes[d * nN + tris[v * F + t]];
+    cplx B[64];
+    oracle_tri_stiff(X, g_re, g_im, B);
+    for (int k = 0; k < 64; ++k) Bmat[t * 64 + k] += B[k];
+  }
+  return 0;
+}
