@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="hex grid nx,ny,nz of the dielectric box (default 100,50,67)")
     ap.add_argument("--forms", default="fp64,mixed", help="comma list of forms to time (fp64, mixed, exact)")
+    ap.add_argument("--sweep", action="store_true",
+                    help="resident frequency sweep: 201 frequencies 8-12 GHz with the two port terms on the workload")
+    ap.add_argument("--sweep-freqs", type=int, default=201)
+    ap.add_argument("--sweep-batch", type=int, default=8, help="frequencies formed per launch (outputs resident)")
     ap.add_argument("--shard", action="store_true",
                     help="strong scaling: one assembly column-sharded over the ranks instead of one replica per rank")
     ap.add_argument("--serving", action="store_true",
@@ -368,6 +372,71 @@ def run_ours(args, rank, world, local_rank):
     return line, wl
 
 
+def run_sweep(args, rank, world, local_rank):
+    """--sweep: K and M of the workload assembled once and kept in HBM, then
+    A(f) = K - k0(f)^2 M + gamma(f) (R_in + R_out) for every frequency (the
+    cached multi-frequency path with TE10 port terms, gamma = j beta(f)),
+    formed --sweep-batch frequencies per launch into resident outputs."""
+    import torch
+
+    from emerge_b200 import workloads as W
+    from emerge_b200.assembly import tet_mass_stiffness_matrices
+    from emerge_b200.mesh import plane_tris
+    from emerge_b200.ranks import max_over_ranks
+    from emerge_b200.robin import RobinTerm
+    from emerge_b200.sweep import FrequencySweep
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = make_workload(args.config, grid=args.grid)
+    f = wl.field
+    z = f.mesh.nodes[2]
+    t0 = time.perf_counter()
+    E, B, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, wl.conductor_tets, precision="fp64", device=dev)
+    ports = [RobinTerm(f, plane_tris(f.mesh, 2, float(z.min())), cmap),
+             RobinTerm(f, plane_tris(f.mesh, 2, float(z.max())), cmap)]
+    sw = FrequencySweep(E, B, cmap, robin=ports)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    freqs = np.linspace(8e9, 12e9, args.sweep_freqs)
+    gam = np.array([W.rect_port_gamma(x) for x in freqs])
+    nb = max(1, min(args.sweep_batch, freqs.size))
+    out = torch.empty((nb, cmap.nnz), dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def sweep():
+        for i0 in range(0, freqs.size, nb):
+            fb = freqs[i0:i0 + nb]
+            g = gam[i0:i0 + nb]
+            sw.form(FrequencySweep.coefficients(fb), out[: fb.size], robin_gamma=np.stack([g, g], axis=1))
+
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        ms = time_steps(sweep, args.steps, args.warmup, stream)
+    E.job.mesh.check_status()
+    ms = max_over_ranks([ms], dev)[0]
+    if rank != 0:
+        return None
+    nnz, nf = cmap.nnz, freqs.size
+    n_launch = -(-nf // nb)
+    bytes_sweep = n_launch * 32 * nnz + nf * 16 * nnz  # K, M read per batch; A written per frequency
+    hbm = (json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+           if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else None) or 6650.0
+    ach = bytes_sweep / (ms * 1e-3) / 1e9
+    return {"metric": "resident frequency sweep: A(f) = K - k0^2 M + gamma(f) R_ports formed per second",
+            "value": world * nf / (ms * 1e-3), "unit": "frequencies/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": wl.name + "_sweep", "tets": f.ntets, "nnz": nnz, "freqs": nf,
+                       "band_hz": [8e9, 12e9], "batch": nb, "port_tris": int(sum(r.n_btris for r in ports)),
+                       "K_M_form": "fp64", "setup_s": setup_s,
+                       "step": f"all {nf} frequencies, {n_launch} form launches + {2 * nf} port-term launches"},
+            "tet_freqs_per_s": world * f.ntets * nf / (ms * 1e-3),
+            "roofline": {"bound": "hbm", "kernel": "k_form_sweep", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                         "frac": ach / hbm, "alg_bytes_per_step": bytes_sweep, "traffic": None},
+            "clocks": sampler.summary(), "gpu_launches": args.steps * (n_launch + 2 * nf)}
+
+
 def run_shard(args, rank, world, local_rank):
     """--shard: the workload's columns split over the ranks (each rank
     assembles the tets touching its edges/faces, no exchange step); one step
@@ -464,6 +533,8 @@ def main():
         line, wl = run_serving(args, rank, world, local_rank), None
     elif args.shard:
         line, wl = run_shard(args, rank, world, local_rank), None
+    elif args.sweep:
+        line, wl = run_sweep(args, rank, world, local_rank), None
     else:
         line, wl = run_ours(args, rank, world, local_rank)
     if rank == 0 and not args.no_cpu_baseline and wl is not None:

@@ -24,6 +24,7 @@ EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
+    "emg_robin_init", "emg_robin_build", "emg_robin_apply",
 )
 
 
@@ -49,6 +50,11 @@ class Plan(ctypes.Structure):
         ("plan_bytes", ctypes.c_size_t),
         ("workspace_bytes", ctypes.c_size_t),
     ]
+
+
+class Robin(ctypes.Structure):
+    _fields_ = [("n_btris", ctypes.c_int64), ("n_slots", ctypes.c_int64), ("n_keys", ctypes.c_int64),
+                ("keys_bytes", ctypes.c_size_t), ("values_bytes", ctypes.c_size_t)]
 
 
 class FormItem(ctypes.Structure):
@@ -97,11 +103,16 @@ def lib():
     L.emg_form_sweep.argtypes = [_P, _P, _P, _I64, ctypes.POINTER(_D), ctypes.c_int, _P, _I64, _P]
     L.emg_form_batch.argtypes = [_P, _P, _P, ctypes.c_int, _P]
     L.emg_plan_order.argtypes = [ctypes.POINTER(Plan), _P, _P, _I64, _P, _P, _P, _P]
+    L.emg_robin_init.argtypes = [_I64, ctypes.POINTER(Robin)]
+    L.emg_robin_build.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P,
+                                  _P]
+    L.emg_robin_apply.argtypes = [ctypes.POINTER(Robin), _P, _P, _D, _D, _P, _I64, _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
                                        ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
     for name in ("emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
-                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order"):
+                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_robin_init", "emg_robin_build",
+                 "emg_robin_apply"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -233,34 +233,40 @@ class LinComb:
     def __init__(self, job: _Job, coef: dict):
         self.job, self.coef = job, dict(coef)
 
-    def _other(self, o) -> dict:
-        if isinstance(o, ElemValues):
+    def _other(self, o):
+        """(job, coef) of the other operand, or NotImplemented."""
+        if isinstance(o, ElemValues) or getattr(o, "_is_robin_term", False):
             o = o._lc()
         if not isinstance(o, LinComb):
             return NotImplemented
-        if o.job is not self.job:
+        if self.job is not None and o.job is not None and o.job is not self.job:
             raise ValueError("element values of different assemblies cannot be combined")
-        return o.coef
+        return (self.job if self.job is not None else o.job), o.coef
 
     def __add__(self, o):
-        oc = self._other(o)
-        if oc is NotImplemented:
+        r = self._other(o)
+        if r is NotImplemented:
             return NotImplemented
+        job, oc = r
         c = dict(self.coef)
         for k, v in oc.items():
             c[k] = c.get(k, 0) + v
-        return LinComb(self.job, c)
+        return LinComb(job, c)
 
     __radd__ = __add__
 
     def __sub__(self, o):
-        oc = self._other(o)
-        if oc is NotImplemented:
+        r = self._other(o)
+        if r is NotImplemented:
             return NotImplemented
+        job, oc = r
         c = dict(self.coef)
         for k, v in oc.items():
             c[k] = c.get(k, 0) - v
-        return LinComb(self.job, c)
+        return LinComb(job, c)
+
+    def __rsub__(self, o):
+        return (-self) + o
 
     def __mul__(self, s):
         if not np.isscalar(s):
@@ -280,7 +286,14 @@ class LinComb:
     def beta(self) -> complex:
         return complex(self.coef.get("M", 0.0))
 
+    @property
+    def robin_terms(self) -> list:
+        """(RobinTerm, gamma) pairs of the combination."""
+        return [(k, complex(v)) for k, v in self.coef.items() if getattr(k, "_is_robin_term", False)]
+
     def __array__(self, dtype=None, copy=None):
+        if self.robin_terms:
+            raise TypeError("a combination with a boundary term has no tet COO layout; use cscmap.to_csc")
         K = np.asarray(ElemValues(self.job, "K"))
         M = np.asarray(ElemValues(self.job, "M"))
         a = self.alpha * K + self.beta * M
@@ -389,9 +402,16 @@ class GpuCSCMapping:
         """Values of to_csc(data) kept on the device (complex128 [nnz])."""
         if isinstance(data, ElemValues):
             data = data._lc()
+        if getattr(data, "_is_robin_term", False):
+            data = data._lc()
         if isinstance(data, LinComb):
-            out = self.assemble_device(data.job, data.alpha, data.beta)
-            data.job.mesh.check_status()
+            if data.job is not None:
+                out = self.assemble_device(data.job, data.alpha, data.beta)
+                data.job.mesh.check_status()
+            else:
+                out = torch.zeros(max(self.nnz, 1), dtype=torch.complex128, device=self.device)
+            for term, gamma in data.robin_terms:
+                term.apply(out, gamma, self)
             return out[: self.nnz]
         arr = np.asarray(data)
         if not np.iscomplexobj(arr):

@@ -538,11 +538,6 @@ size_t plan_layout(emg_plan *p) {
 
 // chunk-order scratch: bounding-box partials and the sort keys (power of two)
 constexpr int BBOX_BLOCKS = 296;
-static int64_t pow2_at_least(int64_t n) {
-  int64_t v = 1;
-  while (v < n) v <<= 1;
-  return v;
-}
 static size_t order_workspace_bytes(const emg_plan *p) {
   return align_up((size_t)BBOX_BLOCKS * 6 * 8 + 64, 256) +
          (size_t)pow2_at_least(n_chunks(p->n_edges, p->n_tris)) * 8;
@@ -645,6 +640,17 @@ int plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, c
   return launch_check("k_chunk_contrib");
 }
 
+int sort_u64(uint64_t *keys, int64_t n2, cudaStream_t s) {
+  if (n2 & (n2 - 1)) return fail(EMG_EINVAL, "sort length %lld is not a power of two", (long long)n2);
+  for (int64_t k = 2; k <= n2; k <<= 1)
+    for (int64_t j = k >> 1; j > 0; j >>= 1) {
+      k_bitonic_step<<<grid_for(n2, 256), 256, 0, s>>>(keys, n2, j, k);
+      const int rc = launch_check("k_bitonic_step");
+      if (rc) return rc;
+    }
+  return EMG_OK;
+}
+
 int plan_order(const emg_plan *p, void *d_plan, const double *nodes, int64_t nN, const int32_t *tets,
                const int32_t *tetids, void *d_ws, cudaStream_t s) {
   const int64_t nch = n_chunks(p->n_edges, p->n_tris);
@@ -664,11 +670,7 @@ int plan_order(const emg_plan *p, void *d_plan, const double *nodes, int64_t nN,
       reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr), reinterpret_cast<const Item *>(plan + p->off_item),
       nodes, nN, tets, p->n_tets, tetids, p->n_assy, box, p->n_edges, p->n_tris, nch, n2, keys);
   if ((rc = launch_check("k_chunk_keys"))) return rc;
-  for (int64_t k = 2; k <= n2; k <<= 1)
-    for (int64_t j = k >> 1; j > 0; j >>= 1) {
-      k_bitonic_step<<<grid_for(n2, 256), 256, 0, s>>>(keys, n2, j, k);
-      if ((rc = launch_check("k_bitonic_step"))) return rc;
-    }
+  if ((rc = sort_u64(keys, n2, s))) return rc;
   k_write_order<<<grid_for(nch, 256), 256, 0, s>>>(keys, nch, reinterpret_cast<int32_t *>(plan + p->off_order));
   return launch_check("k_write_order");
 }

@@ -1,0 +1,251 @@
+// robin.cu -- the Robin (third-kind) boundary term of ports and absorbing
+// boundaries on Nedelec-2 triangles, scattered into A's pattern.
+//
+// Replaces assemble_robin_bc / compute_bc_entries / ned2_tri_stiff
+// (physics/microwave/assembly/robinbc.py:316-451) and the caller's
+// K += field.generate_csc(B_matrix_robin) (assembler.py:576-630,
+// elements/femdata.py:104-118). The triangle block is linear in gamma, so it
+// is built once for gamma = 1 and every frequency adds gamma(f) times it.
+#include "common.cuh"
+
+namespace emg {
+namespace {
+
+// 6-point triangle rule of robinbc.py:189-196 (weights, barycentric L1..L3)
+__constant__ double kTW[6] = {0.10995174365532200, 0.10995174365532200, 0.10995174365532200,
+                              0.22338158967801100, 0.22338158967801100, 0.22338158967801100};
+__constant__ double kTL[3][6] = {
+    {0.81684757298045896, 0.09157621350977101, 0.09157621350977101, 0.10810301816807000, 0.44594849091596500,
+     0.44594849091596500},
+    {0.09157621350977101, 0.81684757298045896, 0.09157621350977101, 0.44594849091596500, 0.10810301816807000,
+     0.44594849091596500},
+    {0.09157621350977004, 0.09157621350977008, 0.81684757298045807, 0.44594849091596500, 0.44594849091596500,
+     0.10810301816807000}};
+
+// position of row `row` in column `col` of the CSC pattern, or -1
+__device__ __forceinline__ int64_t find_in_column(const int32_t *indptr, const int32_t *indices, int64_t col,
+                                                  int32_t row) {
+  int64_t lo = indptr[col], hi = (int64_t)indptr[col + 1] - 1;
+  while (lo <= hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    const int32_t v = indices[mid];
+    if (v == row) return mid;
+    if (v < row) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+// One boundary triangle per thread: the 8x8 block for gamma = 1 in the
+// triangle's own plane (origin at vertex 0, x along edge 0->1), the 2-D
+// Volakis functions ne0, ne2 on the vertex pairs (0,1), (1,2), (0,2) and
+// nf0, nf1 on (0,1,2) at the 6 points, B[a][b] = A * sum_q w_q f_a . f_b
+// (computed for a <= b and mirrored), and each slot's position in A.
+__global__ void __launch_bounds__(128)
+    k_robin_build(const double *nodes, int64_t nN, const int32_t *tris, const int32_t *tri_to_edge, int64_t F,
+                  int64_t E, const int32_t *btris, int64_t nb, const int32_t *indptr, const int32_t *indices,
+                  int64_t N, uint64_t *keys, double2 *vals, int64_t *st) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  uint64_t *my_keys = keys + i * 64;
+  double2 *my_vals = vals + i * 64;
+  const int64_t t = btris[i];
+  bool ok = t >= 0 && t < F;
+  int32_t v[3] = {0, 0, 0}, e[3] = {0, 0, 0};
+  if (ok)
+    for (int k = 0; k < 3; ++k) {
+      v[k] = tris[k * F + t];
+      e[k] = tri_to_edge[k * F + t];
+      ok = ok && v[k] >= 0 && v[k] < nN && e[k] >= 0 && e[k] < E;
+    }
+  if (!ok) {
+    flag(st, EMG_ST_INDEX, i);
+    for (int k = 0; k < 64; ++k) {
+      my_keys[k] = ~0ull;
+      my_vals[k] = make_double2(0.0, 0.0);
+    }
+    return;
+  }
+  double X[3][3];
+  for (int d = 0; d < 3; ++d)
+    for (int k = 0; k < 3; ++k) X[d][k] = nodes[d * nN + v[k]];
+  double e1[3], e2[3], zh[3], xh[3], yh[3];
+  for (int d = 0; d < 3; ++d) {
+    e1[d] = X[d][1] - X[d][0];
+    e2[d] = X[d][2] - X[d][0];
+  }
+  zh[0] = e1[1] * e2[2] - e1[2] * e2[1];
+  zh[1] = e1[2] * e2[0] - e1[0] * e2[2];
+  zh[2] = e1[0] * e2[1] - e1[1] * e2[0];
+  const double nz = sqrt(zh[0] * zh[0] + zh[1] * zh[1] + zh[2] * zh[2]);
+  const double nx = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+  for (int d = 0; d < 3; ++d) {
+    zh[d] /= nz;
+    xh[d] = e1[d] / nx;
+  }
+  yh[0] = zh[1] * xh[2] - zh[2] * xh[1];
+  yh[1] = zh[2] * xh[0] - zh[0] * xh[2];
+  yh[2] = zh[0] * xh[1] - zh[1] * xh[0];
+  const double ny = sqrt(yh[0] * yh[0] + yh[1] * yh[1] + yh[2] * yh[2]);
+  for (int d = 0; d < 3; ++d) yh[d] /= ny;
+  double tx[3], ty[3];
+  for (int k = 0; k < 3; ++k) {
+    double rx = 0.0, ry = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double r = X[d][k] - X[d][0];
+      rx += xh[d] * r;
+      ry += yh[d] * r;
+    }
+    tx[k] = rx;
+    ty[k] = ry;
+  }
+  const double ca0 = tx[1] * ty[2] - ty[1] * tx[2], ca1 = tx[2] * ty[0] - ty[2] * tx[0],
+               ca2 = tx[0] * ty[1] - ty[0] * tx[1];
+  const double cb0 = ty[1] - ty[2], cb1 = ty[2] - ty[0], cb2 = ty[0] - ty[1];
+  const double cc0 = tx[2] - tx[1], cc1 = tx[0] - tx[2], cc2 = tx[1] - tx[0];
+  const double sA = 0.5 * (cb0 * cc1 - cb1 * cc0);
+  const double s2 = 2 * sA;
+  const double ca[3] = {ca0 / s2, ca1 / s2, ca2 / s2}, cb[3] = {cb0 / s2, cb1 / s2, cb2 / s2},
+               cc[3] = {cc0 / s2, cc1 / s2, cc2 / s2};
+  const double area = fabs(sA);
+  if (!(area > 0.0) || !isfinite(area)) flag(st, EMG_ST_DEGENERATE, i);
+  double B[36];
+  for (int k = 0; k < 36; ++k) B[k] = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    const double xs = tx[0] * kTL[0][q] + tx[1] * kTL[1][q] + tx[2] * kTL[2][q];
+    const double ys = ty[0] * kTL[0][q] + ty[1] * kTL[1][q] + ty[2] * kTL[2][q];
+    double L[3];
+    for (int m = 0; m < 3; ++m) L[m] = ca[m] + cb[m] * xs + cc[m] * ys;
+    double f[8][2];
+    const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int a = EI[k], b = EJ[k];
+      const double wx = L[a] * cb[b] - L[b] * cb[a], wy = L[a] * cc[b] - L[b] * cc[a];
+      f[k][0] = wx;
+      f[k][1] = wy;
+      const double s = L[a] - L[b];
+      f[3 + k][0] = s * wx;
+      f[3 + k][1] = s * wy;
+    }
+    f[6][0] = L[0] * (L[1] * cb[2] - L[2] * cb[1]);
+    f[6][1] = L[0] * (L[1] * cc[2] - L[2] * cc[1]);
+    f[7][0] = L[1] * (L[0] * cb[2] - L[2] * cb[0]);
+    f[7][1] = L[1] * (L[0] * cc[2] - L[2] * cc[0]);
+    const double w = kTW[q];
+    int k = 0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+      for (int b = a; b < 8; ++b, ++k) B[k] += (f[a][0] * f[b][0] + f[a][1] * f[b][1]) * w;
+  }
+  // DoFs of the triangle (nedelec2.py:69-79): edges, edges + E, tri + 2E, tri + 2E + F
+  int64_t dof[8];
+  for (int k = 0; k < 3; ++k) {
+    dof[k] = e[k];
+    dof[3 + k] = e[k] + E;
+  }
+  dof[6] = 2 * E + t;
+  dof[7] = 2 * E + F + t;
+  int k = 0;
+  for (int a = 0; a < 8; ++a)
+    for (int b = a; b < 8; ++b, ++k) {
+      const double val = B[k] * area;
+      for (int pass = 0; pass < (a == b ? 1 : 2); ++pass) {
+        const int r = pass ? b : a, c = pass ? a : b;  // slot (r, c): row dof[r] in column dof[c]
+        const int slot = 8 * r + c;
+        int64_t pos = -1;
+        if (dof[c] < N && dof[r] < N) pos = find_in_column(indptr, indices, dof[c], (int32_t)dof[r]);
+        if (pos < 0) flag(st, EMG_ST_INDEX, i);
+        my_keys[slot] = pos < 0 ? ~0ull : (((uint64_t)pos << 32) | (uint64_t)(i * 64 + slot));
+        my_vals[slot] = make_double2(val, 0.0);
+      }
+    }
+}
+
+__global__ void k_pad_keys(uint64_t *keys, int64_t from, int64_t n_keys) {
+  const int64_t k = from + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n_keys) keys[k] = ~0ull;
+}
+
+// A[p] += gamma * (sum of the slots of target p, in slot order); one thread
+// per sorted slot, the first slot of each target sums its run
+__global__ void k_robin_apply(const uint64_t *keys, int64_t n_slots, const double2 *vals, double gr, double gi,
+                              double2 *A, int64_t nnz) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_slots) return;
+  const uint64_t key = keys[i];
+  if (key == ~0ull) return;
+  const uint64_t p = key >> 32;
+  if (i > 0 && (keys[i - 1] >> 32) == p) return;
+  if ((int64_t)p >= nnz) return;
+  double sr = 0.0, si = 0.0;
+  for (int64_t j = i; j < n_slots; ++j) {
+    const uint64_t kj = keys[j];
+    if ((kj >> 32) != p || kj == ~0ull) break;
+    const uint64_t slot = kj & 0xffffffffu;
+    if ((int64_t)slot >= n_slots) continue;
+    const double2 v = vals[slot];
+    sr += v.x;
+    si += v.y;
+  }
+  double2 a = A[p];
+  a.x += gr * sr - gi * si;
+  a.y += gr * si + gi * sr;
+  A[p] = a;
+}
+
+}  // namespace
+}  // namespace emg
+
+using namespace emg;
+
+extern "C" {
+
+int emg_robin_init(int64_t n_btris, emg_robin *r) {
+  if (!r) return fail(EMG_EINVAL, "null robin descriptor");
+  if (n_btris < 0) return fail(EMG_EINVAL, "negative triangle count");
+  if (n_btris * 64 >= (1LL << 32)) return fail(EMG_ERANGE, "more than 2^26 boundary triangles");
+  r->n_btris = n_btris;
+  r->n_slots = n_btris * 64;
+  r->n_keys = n_btris > 0 ? pow2_at_least(r->n_slots) : 0;
+  r->keys_bytes = (size_t)r->n_keys * 8;
+  r->values_bytes = (size_t)r->n_slots * 16;
+  return EMG_OK;
+}
+
+int emg_robin_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                    const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                    const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
+                    int64_t *d_status, emg_stream_t stream) {
+  if (!r) return fail(EMG_EINVAL, "null robin descriptor");
+  if (r->n_btris == 0) return EMG_OK;
+  if (!d_nodes || !d_tris || !d_tri_to_edge || !d_btris || !d_indptr || !d_indices || !d_keys || !d_values)
+    return fail(EMG_EINVAL, "null pointer");
+  if (n_nodes <= 0 || n_tris <= 0 || n_edges <= 0 || N != 2 * n_edges + 2 * n_tris)
+    return fail(EMG_EINVAL, "bad sizes (N must be 2 E + 2 F)");
+  cudaStream_t s = S(stream);
+  k_robin_build<<<grid_for(r->n_btris, 128), 128, 0, s>>>(d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges,
+                                                          d_btris, r->n_btris, d_indptr, d_indices, N, d_keys, static_cast<double2 *>(d_values), d_status);
+  int rc = launch_check("k_robin_build");
+  if (rc) return rc;
+  if (r->n_keys > r->n_slots) {
+    k_pad_keys<<<grid_for(r->n_keys - r->n_slots, 256), 256, 0, s>>>(d_keys, r->n_slots, r->n_keys);
+    if ((rc = launch_check("k_pad_keys"))) return rc;
+  }
+  return sort_u64(d_keys, r->n_keys, s);
+}
+
+int emg_robin_apply(const emg_robin *r, const uint64_t *d_keys, const void *d_values, double gamma_re,
+                    double gamma_im, void *d_A, int64_t nnz, emg_stream_t stream) {
+  if (!r) return fail(EMG_EINVAL, "null robin descriptor");
+  if (r->n_btris == 0) return EMG_OK;
+  if (!d_keys || !d_values || !d_A) return fail(EMG_EINVAL, "null pointer");
+  k_robin_apply<<<grid_for(r->n_slots, 256), 256, 0, S(stream)>>>(
+      d_keys, r->n_slots, static_cast<const double2 *>(d_values), gamma_re, gamma_im, static_cast<double2 *>(d_A),
+      nnz);
+  return launch_check("k_robin_apply");
+}
+
+}  // extern "C"

@@ -192,3 +192,14 @@ def structured_box(nx: int, ny: int, nz: int, size=(22.86e-3, 10.16e-3, 50e-3), 
     tets = corners[_KUHN.T.reshape(-1)].reshape(4, 6, hi.size).transpose(0, 2, 1).reshape(4, -1)
     tets = orient_positive(nodes, tets)
     return nodes, np.ascontiguousarray(tets)
+
+
+def plane_tris(mesh: TetMesh, axis: int, value: float, rtol: float = 1e-9) -> np.ndarray:
+    """Ids of the triangles whose three vertices lie on the plane
+    x[axis] = value (to rtol times the mesh extent along that axis): the
+    surface a port or an absorbing boundary is applied to (the reference
+    selects them by the face's physical tag, mesh3d ``get_triangles``)."""
+    x = mesh.nodes[axis]
+    tol = rtol * max(float(x.max() - x.min()), 1e-300)
+    on = np.abs(x - value) <= tol
+    return np.flatnonzero(on[mesh.tris].all(axis=0)).astype(np.int64)

@@ -1,0 +1,125 @@
+"""Robin (third-kind) boundary term on the GPU: ports, absorbing boundaries
+and surface impedances on boundary triangles.
+
+Reference (physics/microwave/assembly/assembler.py:576-630)::
+
+    B_matrix_robin = field.empty_tri_matrix()
+    B_matrix_robin = assemble_robin_bc(field, B_matrix_robin, tri_ids, gamma)
+    K += field.generate_csc(B_matrix_robin)
+
+Here the term is a lazy object that joins the caller's combination of
+element values::
+
+    R = RobinTerm(field, tri_ids, cscmap)           # built once per surface
+    A = cscmap.to_csc(Evec - Bvec * k0**2 + R * gamma)
+
+``RobinTerm`` builds each triangle's 8x8 block once for gamma = 1 (the block
+is linear in gamma, robinbc.py:316-378) and the position in A of each of its
+64 DoF pairs; every assembly then adds gamma times the blocks into A's values
+on the device, summing each position in a fixed order. Every DoF pair of a
+triangle shares a tet with it, so A's pattern does not change.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+from scipy.sparse import csc_matrix
+
+from . import _lib as L
+from .assembly import GpuCSCMapping, LinComb, _to_dev
+
+__all__ = ["RobinTerm", "assemble_robin_bc"]
+
+
+class RobinTerm:
+    """The boundary term of the triangles ``tri_ids`` (int, into
+    ``field.mesh.tris``) on the pattern of ``cscmap``; ``gamma * term`` is a
+    lazy combination for ``cscmap.to_csc`` / ``to_device``. A triangle listed
+    twice counts twice, as in the reference."""
+
+    _is_robin_term = True
+
+    def __init__(self, field, tri_ids, cscmap: GpuCSCMapping):
+        m = field.mesh
+        ids = np.asarray(tri_ids, dtype=np.int64).ravel()
+        if ids.size and (ids.min() < 0 or ids.max() >= m.n_tris):
+            raise IndexError("triangle id out of range")
+        if int(field.n_field) != cscmap.N:
+            raise ValueError("the mapping belongs to another field")
+        self.cmap = cscmap
+        self.n_btris = int(ids.size)
+        dev = cscmap.device
+        r = L.Robin()
+        L.check(L.lib().emg_robin_init(self.n_btris, L.ctypes.byref(r)))
+        self.desc = r
+        self.d_keys = torch.empty(max(r.n_keys, 1), dtype=torch.int64, device=dev)
+        self.d_vals = torch.empty(max(r.n_slots, 1), dtype=torch.complex128, device=dev)
+        if self.n_btris:
+            nodes = _to_dev(m.nodes, torch.float64, dev)
+            tris = _to_dev(m.tris, torch.int32, dev)
+            t2e = _to_dev(m.tri_to_edge, torch.int32, dev)
+            btris = _to_dev(ids, torch.int32, dev)
+            status = torch.zeros(2, dtype=torch.int64, device=dev)
+            st = L.stream_handle(dev)
+            L.check(L.lib().emg_robin_build(L.ctypes.byref(r), L.ptr(nodes), m.n_nodes, L.ptr(tris), L.ptr(t2e),
+                                            m.n_tris, m.n_edges, L.ptr(btris), L.ptr(cscmap.d_indptr),
+                                            L.ptr(cscmap.d_indices), cscmap.N, L.ptr(self.d_keys),
+                                            L.ptr(self.d_vals), L.ptr(status), st))
+            f, i = L.ctypes.c_int64(), L.ctypes.c_int64()
+            L.check(L.lib().emg_status_read(L.ptr(status), L.ctypes.byref(f), L.ctypes.byref(i), st))
+            if f.value:
+                raise L.EmgMeshError(L.EMG_EMESH, f"boundary triangle {int(ids[i.value]) if 0 <= i.value < ids.size else i.value}: "
+                                     + ("outside the assembled pattern or bad index" if f.value & L.EMG_ST_INDEX
+                                        else "degenerate triangle"))
+
+    def _lc(self) -> LinComb:
+        return LinComb(None, {self: 1.0 + 0.0j})
+
+    def __mul__(self, c):
+        return self._lc() * c
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return self._lc() * -1.0
+
+    def __add__(self, o):
+        return self._lc() + o
+
+    __radd__ = __add__
+
+    def __sub__(self, o):
+        return self._lc() - o
+
+    def __rsub__(self, o):
+        return (-self._lc()) + o
+
+    def apply(self, A: torch.Tensor, gamma: complex, cscmap: GpuCSCMapping | None = None) -> torch.Tensor:
+        """A[p] += gamma * (the term at p) on A's device values (complex128
+        [nnz]); stream-ordered."""
+        if cscmap is not None and cscmap is not self.cmap:
+            raise ValueError("the boundary term was built on another mapping")
+        if A.dtype != torch.complex128 or A.numel() < self.cmap.nnz:
+            raise ValueError("A must be complex128 with nnz values")
+        g = complex(gamma)
+        L.check(L.lib().emg_robin_apply(L.ctypes.byref(self.desc), L.ptr(self.d_keys), L.ptr(self.d_vals), g.real,
+                                        g.imag, L.ptr(A), self.cmap.nnz, L.stream_handle(self.cmap.device)))
+        return A
+
+    def to_device(self, gamma: complex = 1.0) -> torch.Tensor:
+        """gamma times the term on A's pattern (complex128 [nnz], zeros off the
+        boundary), e.g. the P of a frequency sweep."""
+        out = torch.zeros(max(self.cmap.nnz, 1), dtype=torch.complex128, device=self.cmap.device)
+        return self.apply(out, gamma)[: self.cmap.nnz]
+
+    def to_csc(self, gamma: complex = 1.0) -> csc_matrix:
+        """The term alone as a csc_matrix on A's pattern (explicit zeros off the
+        boundary; the reference's generate_csc stores only the nonzeros)."""
+        return self.cmap.to_csc(self * gamma)
+
+
+def assemble_robin_bc(field, tri_ids, gamma: complex, cscmap: GpuCSCMapping) -> LinComb:
+    """``gamma`` times the boundary term of ``tri_ids`` as a lazy combination
+    (the reference's assemble_robin_bc + generate_csc, robinbc.py:436-451,
+    femdata.py:104-118), to be added to the element-value combination."""
+    return RobinTerm(field, tri_ids, cscmap) * gamma

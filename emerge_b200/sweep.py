@@ -5,7 +5,10 @@ The reference caches the COO arrays Evec (K) and Bvec (M) when no material is
 frequency dependent and, per frequency, runs ``to_csc(Evec - Bvec * k0**2)``.
 Here K and M are gathered once into CSC values that stay in HBM, and
 ``emg_form_sweep`` forms A_f = a_f*K + b_f*M (+ c_f*P) for a batch of
-frequencies, reading K, M (and P) once per batch.
+frequencies, reading K, M (and P) once per batch. Port and absorbing
+boundaries (``RobinTerm``, the reference's assemble_robin_bc per frequency,
+assembler.py:576-630) are added as gamma_f times their term, touching only
+the boundary positions.
 """
 from __future__ import annotations
 
@@ -24,7 +27,8 @@ C0 = 299792458.0
 class FrequencySweep:
     """K and M of one assembly resident on the device; A(f) on demand."""
 
-    def __init__(self, E: ElemValues, B: ElemValues, cscmap: GpuCSCMapping, P: torch.Tensor | None = None):
+    def __init__(self, E: ElemValues, B: ElemValues, cscmap: GpuCSCMapping, P: torch.Tensor | None = None,
+                 robin=None):
         if E.job is not B.job:
             raise ValueError("E and B must come from the same tet_mass_stiffness_matrices call")
         self.cscmap = cscmap
@@ -34,6 +38,10 @@ class FrequencySweep:
         if P is not None and (P.dtype != torch.complex128 or P.numel() != cscmap.nnz):
             raise ValueError("P must be complex128 values in the mapping's CSC order")
         self.nnz = cscmap.nnz
+        self.robin = [] if robin is None else (list(robin) if isinstance(robin, (list, tuple)) else [robin])
+        for r in self.robin:
+            if r.cmap is not cscmap:
+                raise ValueError("a boundary term was built on another mapping")
 
     @staticmethod
     def coefficients(freqs, gamma=None) -> np.ndarray:
@@ -48,9 +56,10 @@ class FrequencySweep:
             c[:, 4], c[:, 5] = g.real, g.imag
         return c
 
-    def form(self, coef: np.ndarray, out: torch.Tensor | None = None) -> torch.Tensor:
+    def form(self, coef: np.ndarray, out: torch.Tensor | None = None, robin_gamma=None) -> torch.Tensor:
         """A values for each row of ``coef`` (nf x 6), into out[nf, nnz]
-        (complex128, device); stream-ordered."""
+        (complex128, device), plus robin_gamma[f, j] times boundary term j
+        (robin_gamma: (nf,) for one term or (nf, n_terms)); stream-ordered."""
         coef = np.ascontiguousarray(coef, dtype=np.float64)
         nf = coef.shape[0]
         if out is None:
@@ -60,10 +69,22 @@ class FrequencySweep:
         L.check(L.lib().emg_form_sweep(L.ptr(self.K), L.ptr(self.M), L.ptr(self.P), self.nnz,
                                        coef.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nf, L.ptr(out), self.nnz,
                                        L.stream_handle(self.K.device)))
+        if self.robin:
+            if robin_gamma is None:
+                raise ValueError("the sweep has boundary terms: pass robin_gamma")
+            g = np.asarray(robin_gamma, dtype=np.complex128).reshape(nf, -1)
+            if g.shape[1] != len(self.robin):
+                raise ValueError(f"robin_gamma needs {len(self.robin)} column(s)")
+            for i in range(nf):
+                for j, r in enumerate(self.robin):
+                    r.apply(out[i], complex(g[i, j]))
+        elif robin_gamma is not None:
+            raise ValueError("robin_gamma given but the sweep has no boundary term")
         return out
 
-    def to_csc(self, freq: float, gamma=None) -> csc_matrix:
-        a = self.form(self.coefficients([freq], gamma))[0]
+    def to_csc(self, freq: float, gamma=None, robin_gamma=None) -> csc_matrix:
+        a = self.form(self.coefficients([freq], gamma), robin_gamma=None if robin_gamma is None
+                      else np.reshape(np.asarray(robin_gamma, dtype=np.complex128), (1, -1)))[0]
         host = torch.empty(a.shape, dtype=torch.complex128, pin_memory=True)
         host.copy_(a)
         m = self.cscmap

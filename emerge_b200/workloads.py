@@ -75,6 +75,26 @@ def wr90_dielectric(n=(100, 50, 67), jitter=0.15, seed=1, freq=10e9, block=8) ->
     return Workload("wr90_dielectric", f, er, ur, np.zeros(0, np.int64), freq, tuple(n))
 
 
+def rect_port_gamma(freq: float, width: float = WR90[0], height: float = WR90[1], er: float = 1.0,
+                    mode=(1, 0)) -> complex:
+    """Robin coefficient of a rectangular waveguide port, gamma = j beta with
+    beta = sqrt(er k0^2 - (pi m / width)^2 - (pi n / height)^2)
+    (bcs/port_bcs.py:963-983)."""
+    k0 = 2 * np.pi * freq / C0
+    beta = np.sqrt(er * k0 ** 2 - (np.pi * mode[0] / width) ** 2 - (np.pi * mode[1] / height) ** 2)
+    return 1j * beta
+
+
+def port_tris(wl: Workload) -> np.ndarray:
+    """Triangles of the two waveguide ports of a WR-90 box: the z = 0 and
+    z = length faces."""
+    from .mesh import plane_tris
+
+    m = wl.field.mesh
+    z = m.nodes[2]
+    return np.concatenate([plane_tris(m, 2, float(z.min())), plane_tris(m, 2, float(z.max()))])
+
+
 def alg_bytes(n_nodes: int, n_tets: int, nnz: int, material_bytes_per_tet: int = 16) -> int:
     """Algorithmic bytes of one assembly: nodes + tets + material + int32
     slot->nnz map + segment offsets + complex128 A written."""

@@ -246,6 +246,41 @@ typedef struct {
 int emg_form_batch(const emg_form_item *d_items, const int64_t *d_tile_start, const int32_t *d_n_items, int max_items,
                    emg_stream_t stream);
 
+/* Robin (third-kind) boundary term of ports, absorbing boundaries and
+ * surface impedances on boundary triangles. Replaces assemble_robin_bc /
+ * compute_bc_entries / ned2_tri_stiff (physics/microwave/assembly/
+ * robinbc.py:316-451) and the caller's K += field.generate_csc(B_robin)
+ * (assembler.py:576-630). The triangle block is linear in gamma, so it is
+ * built once (gamma = 1) and each frequency adds gamma(f) times it into A. */
+typedef struct {
+  int64_t n_btris;     /* boundary triangles (a triangle listed twice counts twice) */
+  int64_t n_slots;     /* 64 per triangle: its 8x8 block */
+  int64_t n_keys;      /* power of two >= n_slots: length of the sorted key array */
+  size_t keys_bytes;   /* 8 * n_keys: d_keys of build/apply */
+  size_t values_bytes; /* 16 * n_slots: d_values (complex128) of build/apply */
+} emg_robin;
+
+/* Host-only: sizes for n_btris triangles (fewer than 2^26). */
+int emg_robin_init(int64_t n_btris, emg_robin *robin);
+
+/* Per boundary triangle d_btris[i] (int32 index into tris): its 8x8 block for
+ * gamma = 1 (6-point rule in the triangle's plane, robinbc.py:189-196) and the
+ * position in A (the CSC pattern d_indptr/d_indices of N columns) of each of
+ * its 64 (row, column) DoF pairs; keys sorted by position, then slot, so that
+ * emg_robin_apply sums each position in a fixed order. d_tris, d_tri_to_edge:
+ * int32 [3][n_tris] (sorted vertex ids; edges (v0,v1), (v1,v2), (v0,v2),
+ * mesh3d.py:836-839). A pair outside the pattern (a triangle whose tets are
+ * all excluded) sets EMG_ST_INDEX in d_status and is dropped. */
+int emg_robin_build(const emg_robin *robin, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                    const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                    const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
+                    int64_t *d_status, emg_stream_t stream);
+
+/* d_A[p] += gamma * (sum of the triangle slots at position p) for the nnz
+ * values of A (complex128); stream-ordered, deterministic. */
+int emg_robin_apply(const emg_robin *robin, const uint64_t *d_keys, const void *d_values, double gamma_re,
+                    double gamma_im, void *d_A, int64_t nnz, emg_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,118 @@
+"""Robin (port) boundary term on the GPU against the reference's own output
+(tests/golden/robin.npz) and the oracle. Tolerances: 1e-12 relative
+(Frobenius and max entry) for the term alone and for A + term; the pattern is
+A's, bit-exact."""
+import numpy as np
+import pytest
+
+from emerge_b200 import _lib as L
+from emerge_b200 import workloads as W
+from emerge_b200.assembly import tet_mass_stiffness_matrices
+from emerge_b200.robin import RobinTerm, assemble_robin_bc
+from emerge_b200.sweep import FrequencySweep
+from oracle import oracle as O
+from tests.golden_util import load_npz, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _sparse_rel(mine, ref):
+    d = (mine - ref).tocsc()
+    d.sum_duplicates()
+    nref = np.sqrt((abs(ref.data) ** 2).sum())
+    fro = np.sqrt((abs(d.data) ** 2).sum()) / nref
+    mx = (abs(d.data).max() if d.nnz else 0.0) / abs(ref.data).max()
+    return fro, mx
+
+
+def test_port_term_matches_reference_golden():
+    g = load_npz("robin.npz")
+    wl = W.wr90_air()
+    f = wl.field
+    ids = g["port_ids"]
+    gamma = complex(g["port_gamma"])
+    Bmat = np.zeros(f.mesh.n_tris * 64, np.complex128)
+    Bmat.reshape(-1, 64)[ids] = g["port_B"]
+    ref = O.generate_csc(f, Bmat)
+    _, _, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    R = RobinTerm(f, ids, cmap)
+    mine = R.to_csc(gamma)
+    assert np.array_equal(mine.indptr, cmap.indptr) and np.array_equal(mine.indices, cmap.indices)
+    fro, mx = _sparse_rel(mine, ref)
+    assert fro <= TOL and mx <= TOL, (fro, mx)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
+def test_system_with_ports_matches_oracle(precision, tol):
+    """A = K - k0^2 M + gamma R (drop-in combination) against the oracle's
+    K - k0^2 M plus generate_csc of its Robin entries, on a lossy box."""
+    wl = W.wr90_dielectric(n=(10, 6, 16), seed=5)
+    f = wl.field
+    ids = W.port_tris(wl)
+    k0 = wl.k0
+    gamma = W.rect_port_gamma(wl.freq)
+    E, B, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64), precision=precision)
+    R = RobinTerm(f, ids, cmap)
+    A = cmap.to_csc(E - B * k0 ** 2 + R * gamma)
+    A2 = cmap.to_csc(E - B * k0 ** 2 + assemble_robin_bc(f, ids, gamma, cmap))
+    assert np.array_equal(A.data, A2.data)
+    dE, dB, ocmap = O.tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    from scipy.sparse import csc_matrix
+
+    K = csc_matrix((ocmap.values_lincomb(dE, dB, 1.0, -k0 ** 2), ocmap.indices, ocmap.indptr), shape=A.shape)
+    ref = (K + O.generate_csc(f, O.robin_entries(f, ids, gamma))).tocsc()
+    ref.sort_indices()
+    assert np.array_equal(ref.indptr, A.indptr) and np.array_equal(ref.indices, A.indices)
+    fro, mx = rel_err(A.data, ref.data)
+    assert fro <= tol and mx <= tol, (fro, mx)
+
+
+def test_repeated_triangles_count_twice_and_apply_is_linear():
+    wl = W.wr90_air(n=(6, 4, 10))
+    f = wl.field
+    ids = W.port_tris(wl)
+    _, _, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    R1 = RobinTerm(f, ids, cmap).to_device(1.0).cpu().numpy()
+    R2 = RobinTerm(f, np.concatenate([ids, ids]), cmap).to_device(1.0).cpu().numpy()
+    assert np.allclose(R2, 2 * R1, rtol=1e-15, atol=0)
+    g = 0.3 - 2.5j
+    Rg = RobinTerm(f, ids, cmap).to_device(g).cpu().numpy()
+    assert np.allclose(Rg, g * R1, rtol=1e-15, atol=0)
+    assert np.count_nonzero(R1) > 0 and np.count_nonzero(R1) < cmap.nnz
+
+
+def test_triangle_outside_the_assembled_pattern_raises():
+    wl = W.wr90_air(n=(4, 3, 5))
+    f = wl.field
+    m = f.mesh
+    ids = W.port_tris(wl)[:1]
+    t = int(ids[0])
+    touching = np.flatnonzero((m.tet_to_tri == t).any(axis=0))
+    _, _, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, touching)  # the tri's tet is a conductor
+    with pytest.raises(L.EmgMeshError):
+        RobinTerm(f, ids, cmap)
+    with pytest.raises(IndexError):
+        RobinTerm(f, np.array([m.n_tris]), cmap)
+
+
+def test_sweep_with_port_terms():
+    wl = W.wr90_dielectric(n=(8, 5, 12), seed=2)
+    f = wl.field
+    z = f.mesh.nodes[2]
+    from emerge_b200.mesh import plane_tris
+
+    p1 = plane_tris(f.mesh, 2, float(z.min()))
+    p2 = plane_tris(f.mesh, 2, float(z.max()))
+    E, B, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    R1, R2 = RobinTerm(f, p1, cmap), RobinTerm(f, p2, cmap)
+    sw = FrequencySweep(E, B, cmap, robin=[R1, R2])
+    freqs = np.linspace(8e9, 12e9, 9)
+    gam = np.array([W.rect_port_gamma(x) for x in freqs])
+    A = sw.form(FrequencySweep.coefficients(freqs), robin_gamma=np.stack([gam, gam], axis=1))
+    for i in (0, 4, 8):
+        k0 = 2 * np.pi * freqs[i] / W.C0
+        direct = cmap.to_csc(E - B * k0 ** 2 + R1 * gam[i] + R2 * gam[i]).data
+        assert rel_err(A[i].cpu().numpy(), direct)[0] < 1e-13
+    with pytest.raises(ValueError):
+        sw.form(FrequencySweep.coefficients(freqs))
