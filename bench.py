@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--serving-jobs", type=int, default=50)
     ap.add_argument("--serving-rate", type=float, default=50.0, help="mean arrivals per second")
     ap.add_argument("--serving-budget-gb", type=float, default=120.0)
+    ap.add_argument("--serving-workers", type=int, default=3, help="setup worker threads")
+    ap.add_argument("--serving-batch-nnz", type=float, default=2 ** 28, help="nonzeros per form batch (cap)")
     return ap.parse_args()
 
 
@@ -486,7 +488,8 @@ def run_serving(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     jobs, arr = synthetic_stream(args.serving_jobs, args.serving_rate, seed=rank)
     warm, warr = synthetic_stream(3, 1000.0, tets=(5_000, 50_000), n_freq=(1, 4), seed=1000 + rank)
-    with AssemblyServer(device=local_rank, budget_bytes=args.serving_budget_gb * 1e9, precision="mixed") as srv:
+    with AssemblyServer(device=local_rank, budget_bytes=args.serving_budget_gb * 1e9, precision="mixed",
+                        setup_workers=args.serving_workers, max_batch_nnz=int(args.serving_batch_nnz)) as srv:
         run_stream(srv, warm, warr)
         srv.n_batches = srv.n_items = 0
         srv.peak_in_use = 0
@@ -505,7 +508,10 @@ def run_serving(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mixed", "data": "synthetic",
             "config": {"workload": "serving_stream", "jobs": r["jobs"], "rate_per_s": args.serving_rate,
                        "tets": "log-uniform [5k, 500k]", "freqs": "U{1..64} in U[1, 40] GHz",
-                       "budget_gb": args.serving_budget_gb, "parallelism": f"replicas x{world}"},
+                       "budget_gb": args.serving_budget_gb, "setup_workers": args.serving_workers,
+                       "batch_nnz_cap": int(args.serving_batch_nnz),
+                       "alloc_conf": os.environ.get("PYTORCH_CUDA_ALLOC_CONF", ""),
+                       "parallelism": f"replicas x{world}"},
             "serving": r}
     return line if rank == 0 else None
 

@@ -46,8 +46,25 @@ def _device(device) -> torch.device:
     return d
 
 
-def _to_dev(a: np.ndarray, dtype: torch.dtype, dev: torch.device) -> torch.Tensor:
-    return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dtype, non_blocking=False)
+_NP = {torch.float64: np.float64, torch.int32: np.int32, torch.int64: np.int64, torch.complex128: np.complex128,
+       torch.complex64: np.complex64, torch.uint8: np.uint8}
+
+
+def _empty(numel: int, dtype: torch.dtype, dev: torch.device, alloc=None) -> torch.Tensor:
+    """Device tensor of numel elements: from ``alloc(numel, dtype)`` when the
+    caller manages device memory itself (e.g. a serving arena), else torch."""
+    if alloc is not None:
+        return alloc(int(numel), dtype)
+    return torch.empty(int(numel), dtype=dtype, device=dev)
+
+
+def _to_dev(a: np.ndarray, dtype: torch.dtype, dev: torch.device, alloc=None) -> torch.Tensor:
+    if alloc is None:
+        return torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=dtype, non_blocking=False)
+    h = np.ascontiguousarray(a, dtype=_NP[dtype])
+    t = alloc(int(h.size), dtype)
+    t.copy_(torch.from_numpy(h.reshape(-1)))
+    return t.view(h.shape)
 
 
 def _prec(precision: str) -> int:
@@ -61,10 +78,11 @@ def _prec(precision: str) -> int:
 class DeviceMesh:
     """Device copies of the mesh arrays the path reads (int32 SoA)."""
 
-    def __init__(self, field, conductor_tets=None, device=None):
+    def __init__(self, field, conductor_tets=None, device=None, alloc=None):
         dev = _device(device)
         mesh = field.mesh
         self.device = dev
+        self.alloc = alloc
         self.n_nodes = int(mesh.nodes.shape[1])
         self.n_tets = int(mesh.tets.shape[1])
         self.n_edges = int(mesh.edges.shape[1])
@@ -75,17 +93,19 @@ class DeviceMesh:
         dc = np.asarray(field.dofcodes3d)
         if dc.shape != (20,) or not np.array_equal(dc, [64] * 6 + [66] * 6 + [128] * 4 + [129] * 4):
             raise ValueError(f"unsupported dofcodes {dc.tolist()} (expected SECOND_MIXED_VOLAKIS)")
-        self.nodes = _to_dev(mesh.nodes, torch.float64, dev)
-        self.tets = _to_dev(mesh.tets, torch.int32, dev)
+        self.nodes = _to_dev(mesh.nodes, torch.float64, dev, alloc)
+        self.tets = _to_dev(mesh.tets, torch.int32, dev, alloc)
         self.tetids_host = _tet_assy(self.n_tets, conductor_tets)
         self.n_assy = int(self.tetids_host.shape[0]) if self.tetids_host is not None else self.n_tets
-        self.tetids = _to_dev(self.tetids_host, torch.int32, dev) if self.tetids_host is not None else None
+        self.tetids = _to_dev(self.tetids_host, torch.int32, dev, alloc) if self.tetids_host is not None else None
         self._field = field
-        self.status = torch.zeros(2, dtype=torch.int64, device=dev)
+        self.status = _empty(2, torch.int64, dev, alloc)
+        self.status.zero_()
 
     def topology(self):
         mesh = self._field.mesh
-        return (_to_dev(mesh.tet_to_edge, torch.int32, self.device), _to_dev(mesh.tet_to_tri, torch.int32, self.device))
+        return (_to_dev(mesh.tet_to_edge, torch.int32, self.device, self.alloc),
+                _to_dev(mesh.tet_to_tri, torch.int32, self.device, self.alloc))
 
     def check_status(self, stream=None):
         f, i = L.ctypes.c_int64(), L.ctypes.c_int64()
@@ -135,7 +155,7 @@ def _is_identity(t: np.ndarray) -> bool:
 class DeviceMaterial:
     """Per-tet er, ur in the compact layout of their kind (see emg_material)."""
 
-    def __init__(self, er: np.ndarray, ur: np.ndarray, n_tets: int, device):
+    def __init__(self, er: np.ndarray, ur: np.ndarray, n_tets: int, device, alloc=None):
         er = np.asarray(er)
         ur = np.asarray(ur)
         if er.shape != (3, 3, n_tets) or ur.shape != (3, 3, n_tets):
@@ -148,11 +168,11 @@ class DeviceMaterial:
 
         def pack(t):
             if kind == L.EMG_MAT_ISO:
-                return _to_dev(t[0, 0].astype(np.complex128, copy=False), torch.complex128, device)
+                return _to_dev(t[0, 0].astype(np.complex128, copy=False), torch.complex128, device, alloc)
             if kind == L.EMG_MAT_DIAG:
                 return _to_dev(np.stack([t[0, 0], t[1, 1], t[2, 2]]).astype(np.complex128, copy=False),
-                               torch.complex128, device)
-            return _to_dev(t.astype(np.complex128, copy=False), torch.complex128, device)
+                               torch.complex128, device, alloc)
+            return _to_dev(t.astype(np.complex128, copy=False), torch.complex128, device, alloc)
 
         self.er = pack(er)
         self.ur = None if ur_id else pack(ur)
@@ -318,15 +338,16 @@ class GpuCSCMapping:
         plan = L.Plan()
         L.check(lib.emg_plan_init(m.n_tets, m.n_assy, m.n_edges, m.n_tris, L.ctypes.byref(plan)))
         self.plan = plan
-        self.d_plan = torch.empty(max(plan.plan_bytes, 1), dtype=torch.uint8, device=m.device)
-        ws = torch.empty(max(plan.workspace_bytes, 1), dtype=torch.uint8, device=m.device)
-        self.d_indptr = torch.empty(self.N + 1, dtype=torch.int32, device=m.device)
+        self.alloc = m.alloc
+        self.d_plan = _empty(max(plan.plan_bytes, 1), torch.uint8, m.device, m.alloc)
+        ws = _empty(max(plan.workspace_bytes, 1), torch.uint8, m.device, m.alloc)
+        self.d_indptr = _empty(self.N + 1, torch.int32, m.device, m.alloc)
         t2e, t2t = m.topology()
         st = L.stream_handle(m.device)
         L.check(lib.emg_plan_build(L.ctypes.byref(plan), L.ptr(m.tets), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids),
                                    L.ptr(self.d_plan), L.ptr(ws), L.ptr(self.d_indptr), L.ptr(m.status), st))
         self.nnz = int(plan.nnz)
-        self.d_indices = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=m.device)
+        self.d_indices = _empty(max(self.nnz, 1), torch.int32, m.device, m.alloc)
         L.check(lib.emg_plan_finish(L.ctypes.byref(plan), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids),
                                     L.ptr(self.d_plan), L.ptr(self.d_indptr), L.ptr(self.d_indices),
                                     L.ptr(m.status), st))
@@ -367,7 +388,7 @@ class GpuCSCMapping:
     def workspace(self, precision: int) -> torch.Tensor:
         need = L.lib().emg_assemble_workspace_size(self.n_assy, precision)
         if self._ws is None or self._ws.numel() < need:
-            self._ws = torch.empty(max(need, 1), dtype=torch.uint8, device=self.device)
+            self._ws = _empty(max(need, 1), torch.uint8, self.device, self.alloc)
         return self._ws
 
     def assemble_device(self, job: _Job, alpha: complex, beta: complex, out: torch.Tensor | None = None):
@@ -376,7 +397,7 @@ class GpuCSCMapping:
         self._check_job(job)
         m = job.mesh
         if out is None:
-            out = torch.empty(max(self.nnz, 1), dtype=torch.complex128, device=self.device)
+            out = _empty(max(self.nnz, 1), torch.complex128, self.device, self.alloc)
         ws = self.workspace(job.precision)
         mat = job.mat.struct()
         m.reset_status()

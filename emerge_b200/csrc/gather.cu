@@ -263,7 +263,9 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
 
 int launch_form_batch(const emg_form_item *items, const int64_t *tile_start, const int32_t *n_items, int max_items,
                       cudaStream_t s) {
-  k_form_batch<<<persistent_ctas(4), 256, 0, s>>>(items, tile_start, n_items, max_items);
+  // many short-lived CTAs (a few tiles each) rather than a persistent grid,
+  // so that kernels of higher-priority streams are scheduled between them
+  k_form_batch<<<persistent_ctas(16), 256, 0, s>>>(items, tile_start, n_items, max_items);
   return launch_check("k_form_batch");
 }
 

@@ -11,8 +11,11 @@ device (latency = arrival -> last A(f) ready).
   pattern + gather plan, K and M assembled once and kept resident.
 * Batching: one batcher thread packs ready (job, frequency) items of every
   active job - jobs that arrived while others were running included - into a
-  single persistent-grid launch (``emg_form_batch``). The launch and the copy
-  of its descriptor are captured once in a CUDA graph and replayed per batch.
+  single launch (``emg_form_batch``); jobs with the least remaining work go
+  first and a batch is capped in size so that setup kernels (on
+  higher-priority streams) get the GPU between batches. The launch and the
+  copy of its descriptor are captured once in a CUDA graph and replayed per
+  batch.
   Each job has a few output slots; an item writes one slot and frees it when
   the result has been handed over.
 
@@ -55,6 +58,7 @@ class AssemblyJob:
     t_setup: float = 0.0
     t_done: float = 0.0
     results: dict = dfield(default_factory=dict)
+    setup_parts: dict = dfield(default_factory=dict)
     error: BaseException | None = None
     done: threading.Event = dfield(default_factory=threading.Event)
 
@@ -67,16 +71,79 @@ class AssemblyJob:
         return int(self.field.ntets)
 
     def footprint(self, precision: int, slots: int) -> int:
-        """HBM bytes this job holds while active (plan, pattern, K, M, element
-        workspace, output slots, mesh and materials), an upper estimate."""
+        """Upper bound of the device bytes this job holds while active: mesh,
+        topology, plan and its workspace, pattern, materials (full tensors
+        assumed), element workspace, K, M and the output slots, each rounded
+        up to the arena alignment."""
         m = self.field.mesh
-        nT, E, F = m.n_tets, m.n_edges, m.n_tris
+        nT, nN, E, F = m.n_tets, m.n_nodes, m.n_edges, m.n_tris
+        nA = nT - int(np.unique(np.asarray(self.conductor_tets)).size)
+        p = L.Plan()
+        L.check(L.lib().emg_plan_init(nT, nA, E, F, L.ctypes.byref(p)))
         nnz = nnz_of(nT, E, F)
-        items = 10 * nT
-        plan = 4 * (E + F) * 2 + items * (16 + 40 + 40 + 160)
-        pattern = 4 * (2 * E + 2 * F + 1) + 4 * nnz
-        values = 210 * nT * (8 if precision == L.EMG_MIXED else 16)
-        return int(plan + pattern + values + (2 + slots) * 16 * nnz + 24 * m.n_nodes + 64 * nT + (64 << 20))
+        sizes = [24 * nN, 16 * nT, 4 * nA, 16, 24 * nT, 16 * nT, p.plan_bytes, p.workspace_bytes,
+                 4 * (2 * E + 2 * F + 1), 4 * nnz, 144 * nT, 144 * nT,
+                 L.lib().emg_assemble_workspace_size(nA, precision)] + [16 * nnz] * (2 + slots)
+        return int(sum(-(-x // ARENA_ALIGN) * ARENA_ALIGN for x in sizes))
+
+
+ARENA_ALIGN = 256
+
+
+class DeviceArena:
+    """One device buffer allocated when the server starts, carved into one
+    contiguous block per admitted job (first fit, freed blocks coalesce).
+    Serving then calls no cudaMalloc / cudaFree, which would synchronise the
+    device, and admission is exact: a job starts when its block fits."""
+
+    def __init__(self, nbytes: int, device):
+        self.size = -(-int(nbytes) // ARENA_ALIGN) * ARENA_ALIGN
+        self.buf = torch.empty(max(self.size, ARENA_ALIGN), dtype=torch.uint8, device=device)
+        self._free = [(0, self.size)]  # (offset, bytes), sorted by offset
+        self.in_use = 0
+        self.peak = 0
+
+    def reserve(self, nbytes: int):
+        """Offset of a free block of nbytes (rounded up), or None."""
+        n = -(-int(nbytes) // ARENA_ALIGN) * ARENA_ALIGN
+        for i, (off, sz) in enumerate(self._free):
+            if sz >= n:
+                if sz == n:
+                    self._free.pop(i)
+                else:
+                    self._free[i] = (off + n, sz - n)
+                self.in_use += n
+                self.peak = max(self.peak, self.in_use)
+                return ArenaBlock(self, off, n)
+        return None
+
+    def release(self, block: "ArenaBlock") -> None:
+        off, n = block.off, block.n
+        i = 0
+        while i < len(self._free) and self._free[i][0] < off:
+            i += 1
+        self._free.insert(i, (off, n))
+        if i + 1 < len(self._free) and self._free[i][0] + self._free[i][1] == self._free[i + 1][0]:
+            self._free[i] = (off, n + self._free.pop(i + 1)[1])
+        if i > 0 and self._free[i - 1][0] + self._free[i - 1][1] == self._free[i][0]:
+            self._free[i - 1] = (self._free[i - 1][0], self._free[i - 1][1] + self._free.pop(i)[1])
+        self.in_use -= n
+
+
+class ArenaBlock:
+    """A job's block; calling it hands out aligned tensors front to back."""
+
+    def __init__(self, arena: DeviceArena, off: int, n: int):
+        self.arena, self.off, self.n, self.top = arena, off, n, 0
+
+    def __call__(self, numel: int, dtype: torch.dtype) -> torch.Tensor:
+        nbytes = int(numel) * dtype.itemsize
+        start = self.top
+        self.top = start + -(-max(nbytes, 1) // ARENA_ALIGN) * ARENA_ALIGN
+        if self.top > self.n:
+            raise MemoryError("job block overflow (footprint bound violated)")
+        o = self.off + start
+        return self.arena.buf[o:o + nbytes].view(dtype)
 
 
 def nnz_of(n_tets: int, n_edges: int, n_tris: int) -> int:
@@ -104,16 +171,17 @@ class AssemblyServer:
     """Continuous-batching assembly server (see module docstring)."""
 
     def __init__(self, device=0, budget_bytes: float = 120e9, setup_workers: int = 3, precision: str = "mixed",
-                 slots_per_job: int = 4, max_items: int = 512, use_graph: bool = True):
+                 slots_per_job: int = 4, max_items: int = 512, use_graph: bool = True, max_batch_nnz: int = 1 << 28):
         self.dev = torch.device("cuda", device)
         self.budget = int(budget_bytes)
         self.precision = _prec(precision)
         self.slots = slots_per_job
         self.max_items = max_items
         self.use_graph = use_graph
+        self.max_batch_nnz = int(max_batch_nnz)
         self._lock = threading.Lock()
         self._pending: deque[AssemblyJob] = deque()
-        self._in_use = 0
+        self.arena = DeviceArena(self.budget, self.dev)
         self.peak_in_use = 0
         self._setup_q: queue.Queue = queue.Queue()
         self._active: list[_Active] = []
@@ -135,7 +203,7 @@ class AssemblyServer:
         self._graph = None
         if use_graph:
             # an empty batch (n = 0) initialises the launch path, then the
-            # descriptor copies + the persistent launch are captured once
+            # descriptor copies + the batch launch are captured once
             with torch.cuda.stream(self._batch_stream):
                 self._issue()
             self._batch_stream.synchronize()
@@ -170,6 +238,7 @@ class AssemblyServer:
         for t in self._threads:
             t.join(timeout=30)
         self._graph = None
+        self.arena = None
 
     def __enter__(self):
         return self
@@ -179,7 +248,7 @@ class AssemblyServer:
 
     @property
     def in_use(self) -> int:
-        return self._in_use
+        return self.arena.in_use
 
     # ------------------------------------------------------------ admission
     def _admit(self) -> None:
@@ -188,17 +257,17 @@ class AssemblyServer:
             while self._pending:
                 j = self._pending[0]
                 need = j.footprint(self.precision, self.slots)
-                if need > self.budget:
+                if need > self.arena.size:
                     self._pending.popleft()
-                    j.error = MemoryError(f"job {j.job_id} needs {need} B, over the {self.budget} B budget")
+                    j.error = MemoryError(f"job {j.job_id} needs {need} B, over the {self.arena.size} B budget")
                     j.done.set()
                     continue
-                if self._in_use + need > self.budget:
-                    break  # FIFO: wait for memory
+                block = self.arena.reserve(need)
+                if block is None:
+                    break  # FIFO: wait for a block
                 self._pending.popleft()
-                self._in_use += need
-                self.peak_in_use = max(self.peak_in_use, self._in_use)
-                j._need = need
+                self.peak_in_use = max(self.peak_in_use, self.arena.in_use)
+                j._block = block
                 j.t_admitted = time.perf_counter()
                 admitted.append(j)
         for j in admitted:
@@ -209,7 +278,8 @@ class AssemblyServer:
         act.K = act.M = act.cmap = None
         act.out = []
         with self._lock:
-            self._in_use -= j._need
+            self.arena.release(j._block)
+            j._block = None
             self._active.remove(act)
         j.t_done = time.perf_counter()
         self.completed.append(j)
@@ -219,7 +289,8 @@ class AssemblyServer:
     # ------------------------------------------------------------ setup workers
     def _setup_loop(self) -> None:
         torch.cuda.set_device(self.dev)
-        stream = torch.cuda.Stream(self.dev)
+        # setup kernels take the GPU ahead of queued batch tiles
+        stream = torch.cuda.Stream(self.dev, priority=-1)
         while not self._stop.is_set():
             j = self._setup_q.get()
             if j is None:
@@ -227,23 +298,30 @@ class AssemblyServer:
             act = _Active(j, self.slots)
             try:
                 with torch.cuda.stream(stream):
-                    dmesh = DeviceMesh(j.field, j.conductor_tets, self.dev)
+                    tp = [time.perf_counter()]
+                    blk = j._block
+                    dmesh = DeviceMesh(j.field, j.conductor_tets, self.dev, alloc=blk)
+                    tp.append(time.perf_counter())
                     cmap = GpuCSCMapping(dmesh)
-                    dmat = DeviceMaterial(j.er, j.ur, dmesh.n_tets, self.dev)
+                    tp.append(time.perf_counter())
+                    dmat = DeviceMaterial(j.er, j.ur, dmesh.n_tets, self.dev, alloc=blk)
+                    tp.append(time.perf_counter())
                     job = _Job(dmesh, dmat, self.precision)
                     act.K = cmap.assemble_device(job, 1.0 + 0j, 0j)
                     act.M = cmap.assemble_device(job, 0j, 1.0 + 0j)
-                    cmap._ws = None  # element workspace no longer needed
-                    act.out = [torch.empty(max(cmap.nnz, 1), dtype=torch.complex128, device=self.dev)
-                               for _ in range(self.slots)]
+                    act.out = [blk(max(cmap.nnz, 1), torch.complex128) for _ in range(self.slots)]
                     act.cmap = cmap
                     stream.synchronize()
                     dmesh.check_status()
+                    tp.append(time.perf_counter())
+                    j.setup_parts = dict(zip(("upload", "pattern", "material", "K_M"), np.diff(tp)))
                 j.t_setup = time.perf_counter()
             except BaseException as e:  # reported on the job, the server keeps serving
                 j.error = e
+                stream.synchronize()
                 with self._lock:
-                    self._in_use -= j._need
+                    self.arena.release(j._block)
+                    j._block = None
                 j.done.set()
                 self._admit()
                 continue
@@ -253,13 +331,20 @@ class AssemblyServer:
 
     # ------------------------------------------------------------ batcher
     def _collect(self):
-        batch = []
+        """Items of the next batch: jobs with the least remaining work first
+        (short jobs finish in the first batches), at most max_items items and
+        about max_batch_nnz nonzeros, so that a batch stays short and setup
+        work on the other streams gets the GPU between batches."""
+        batch, work = [], 0
         with self._lock:
-            for act in self._active:
+            order = sorted(self._active, key=lambda a: (len(a.job.freqs) - a.next_f) * a.cmap.nnz)
+            for act in order:
                 j = act.job
-                while act.free_slots and act.next_f < len(j.freqs) and len(batch) < self.max_items:
+                while (act.free_slots and act.next_f < len(j.freqs) and len(batch) < self.max_items
+                       and (not batch or work + act.cmap.nnz <= self.max_batch_nnz)):
                     batch.append((act, act.next_f, act.free_slots.popleft()))
                     act.next_f += 1
+                    work += act.cmap.nnz
         return batch
 
     def _launch(self, batch) -> None:
@@ -323,9 +408,20 @@ class AssemblyServer:
 
 
 def latency_summary(jobs) -> dict:
+    """Latency percentiles (arrival -> last A(f) ready), and the same split
+    into admission wait, setup (upload, pattern, K, M) and forming."""
     lat = np.array([j.latency for j in jobs]) * 1e3
-    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "jobs": int(lat.size)}
+    out = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "jobs": int(lat.size)}
+    for name, a, b in (("wait", "arrival", "t_admitted"), ("setup", "t_admitted", "t_setup"),
+                       ("form", "t_setup", "t_done")):
+        d = np.array([getattr(j, b) - getattr(j, a) for j in jobs]) * 1e3
+        out[f"{name}_p50_ms"] = float(np.percentile(d, 50))
+        out[f"{name}_p99_ms"] = float(np.percentile(d, 99))
+    parts = [j.setup_parts for j in jobs if j.setup_parts]
+    if parts:
+        out["setup_parts_mean_ms"] = {k: 1e3 * float(np.mean([p[k] for p in parts])) for k in parts[0]}
+    return out
 
 
 # ---------------------------------------------------------------- synthetic stream

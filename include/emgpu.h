@@ -235,9 +235,9 @@ typedef struct {
   double coef[6];
 } emg_form_item;
 
-/* Persistent-grid form of a batch of (job, frequency) items that may belong
- * to different meshes: the items are split into tiles of 32768 nonzeros and
- * one launch of (SM count x 4) CTAs walks all tiles. The item count and the
+/* Form of a batch of (job, frequency) items that may belong to different
+ * meshes in one launch: the items are split into tiles of 32768 nonzeros and
+ * a fixed grid of (SM count x 16) CTAs walks all tiles, a few per CTA. The item count and the
  * tile offsets are read from DEVICE memory (*d_n_items, d_tile_start[n+1]),
  * so one captured CUDA graph (a host-to-device copy of a new batch followed
  * by this launch) can be replayed for every batch. Serving-engine entry

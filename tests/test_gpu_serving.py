@@ -106,13 +106,13 @@ def test_job_over_budget_is_rejected():
 
 def test_mixed_precision_jobs_alone_vs_mix():
     specs = _specs()[:3]
-    with AssemblyServer(precision="mixed") as srv:
+    with AssemblyServer(precision="mixed", budget_bytes=8e9) as srv:
         ref = []
         for j in _jobs(specs):
             srv.submit(j)
             srv.wait([j], timeout=120)
             ref.append(j)
-    with AssemblyServer(precision="mixed", max_items=4, slots_per_job=2) as srv:
+    with AssemblyServer(precision="mixed", budget_bytes=8e9, max_items=4, slots_per_job=2) as srv:
         jobs = [srv.submit(j) for j in _jobs(specs)]
         srv.wait(jobs, timeout=120)
     _assert_same(jobs, ref)
