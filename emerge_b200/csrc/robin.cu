@@ -36,6 +36,103 @@ __device__ __forceinline__ int64_t find_in_column(const int32_t *indptr, const i
   return -1;
 }
 
+// The triangle's own frame (origin at vertex 0, x along edge 0->1, z the
+// normal; construct_local_vertices, robinbc.py:165-183) and its barycentric
+// coefficients (tri_coefficients :200-221). Returns the area.
+struct TriFrame {
+  double xh[3], yh[3], tx[3], ty[3], ca[3], cb[3], cc[3];
+};
+
+__device__ double tri_frame(const double *nodes, int64_t nN, const int32_t v[3], TriFrame &T) {
+  double X[3][3];
+  for (int d = 0; d < 3; ++d)
+    for (int k = 0; k < 3; ++k) X[d][k] = nodes[d * nN + v[k]];
+  double e1[3], e2[3], zh[3];
+  for (int d = 0; d < 3; ++d) {
+    e1[d] = X[d][1] - X[d][0];
+    e2[d] = X[d][2] - X[d][0];
+  }
+  zh[0] = e1[1] * e2[2] - e1[2] * e2[1];
+  zh[1] = e1[2] * e2[0] - e1[0] * e2[2];
+  zh[2] = e1[0] * e2[1] - e1[1] * e2[0];
+  const double nz = sqrt(zh[0] * zh[0] + zh[1] * zh[1] + zh[2] * zh[2]);
+  const double nx = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+  for (int d = 0; d < 3; ++d) {
+    zh[d] /= nz;
+    T.xh[d] = e1[d] / nx;
+  }
+  T.yh[0] = zh[1] * T.xh[2] - zh[2] * T.xh[1];
+  T.yh[1] = zh[2] * T.xh[0] - zh[0] * T.xh[2];
+  T.yh[2] = zh[0] * T.xh[1] - zh[1] * T.xh[0];
+  const double ny = sqrt(T.yh[0] * T.yh[0] + T.yh[1] * T.yh[1] + T.yh[2] * T.yh[2]);
+  for (int d = 0; d < 3; ++d) T.yh[d] /= ny;
+  for (int k = 0; k < 3; ++k) {
+    double rx = 0.0, ry = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double r = X[d][k] - X[d][0];
+      rx += T.xh[d] * r;
+      ry += T.yh[d] * r;
+    }
+    T.tx[k] = rx;
+    T.ty[k] = ry;
+  }
+  const double *tx = T.tx, *ty = T.ty;
+  const double a0 = tx[1] * ty[2] - ty[1] * tx[2], a1 = tx[2] * ty[0] - ty[2] * tx[0], a2 = tx[0] * ty[1] - ty[0] * tx[1];
+  const double b0 = ty[1] - ty[2], b1 = ty[2] - ty[0], b2 = ty[0] - ty[1];
+  const double c0 = tx[2] - tx[1], c1 = tx[0] - tx[2], c2 = tx[1] - tx[0];
+  const double sA = 0.5 * (b0 * c1 - b1 * c0);
+  const double s2 = 2 * sA;
+  T.ca[0] = a0 / s2, T.ca[1] = a1 / s2, T.ca[2] = a2 / s2;
+  T.cb[0] = b0 / s2, T.cb[1] = b1 / s2, T.cb[2] = b2 / s2;
+  T.cc[0] = c0 / s2, T.cc[1] = c1 / s2, T.cc[2] = c2 / s2;
+  return fabs(sA);
+}
+
+// the 8 Volakis functions (ne0, ne2 on (0,1), (1,2), (0,2); nf0, nf1) at point q
+__device__ __forceinline__ void tri_functions(const TriFrame &T, int q, double f[8][2]) {
+  const double xs = T.tx[0] * kTL[0][q] + T.tx[1] * kTL[1][q] + T.tx[2] * kTL[2][q];
+  const double ys = T.ty[0] * kTL[0][q] + T.ty[1] * kTL[1][q] + T.ty[2] * kTL[2][q];
+  double L[3];
+  for (int m = 0; m < 3; ++m) L[m] = T.ca[m] + T.cb[m] * xs + T.cc[m] * ys;
+  const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int a = EI[k], b = EJ[k];
+    const double wx = L[a] * T.cb[b] - L[b] * T.cb[a], wy = L[a] * T.cc[b] - L[b] * T.cc[a];
+    f[k][0] = wx;
+    f[k][1] = wy;
+    const double s = L[a] - L[b];
+    f[3 + k][0] = s * wx;
+    f[3 + k][1] = s * wy;
+  }
+  f[6][0] = L[0] * (L[1] * T.cb[2] - L[2] * T.cb[1]);
+  f[6][1] = L[0] * (L[1] * T.cc[2] - L[2] * T.cc[1]);
+  f[7][0] = L[1] * (L[0] * T.cb[2] - L[2] * T.cb[0]);
+  f[7][1] = L[1] * (L[0] * T.cc[2] - L[2] * T.cc[0]);
+}
+
+// DoFs of the triangle (nedelec2.py:69-79): edges, edges + E, tri + 2E, tri + 2E + F
+__device__ __forceinline__ void tri_dofs(const int32_t e[3], int64_t t, int64_t E, int64_t F, int64_t dof[8]) {
+  for (int k = 0; k < 3; ++k) {
+    dof[k] = e[k];
+    dof[3 + k] = e[k] + E;
+  }
+  dof[6] = 2 * E + t;
+  dof[7] = 2 * E + F + t;
+}
+
+// load and check a boundary triangle's vertices and edges
+__device__ __forceinline__ bool tri_load(const int32_t *tris, const int32_t *tri_to_edge, int64_t F, int64_t nN,
+                                         int64_t E, int64_t t, int32_t v[3], int32_t e[3]) {
+  bool ok = t >= 0 && t < F;
+  for (int k = 0; k < 3; ++k) {
+    v[k] = ok ? tris[k * F + t] : 0;
+    e[k] = ok ? tri_to_edge[k * F + t] : 0;
+    ok = ok && v[k] >= 0 && v[k] < nN && e[k] >= 0 && e[k] < E;
+  }
+  return ok;
+}
+
 // One boundary triangle per thread: the 8x8 block for gamma = 1 in the
 // triangle's own plane (origin at vertex 0, x along edge 0->1), the 2-D
 // Volakis functions ne0, ne2 on the vertex pairs (0,1), (1,2), (0,2) and
@@ -50,15 +147,8 @@ __global__ void __launch_bounds__(128)
   uint64_t *my_keys = keys + i * 64;
   double2 *my_vals = vals + i * 64;
   const int64_t t = btris[i];
-  bool ok = t >= 0 && t < F;
-  int32_t v[3] = {0, 0, 0}, e[3] = {0, 0, 0};
-  if (ok)
-    for (int k = 0; k < 3; ++k) {
-      v[k] = tris[k * F + t];
-      e[k] = tri_to_edge[k * F + t];
-      ok = ok && v[k] >= 0 && v[k] < nN && e[k] >= 0 && e[k] < E;
-    }
-  if (!ok) {
+  int32_t v[3], e[3];
+  if (!tri_load(tris, tri_to_edge, F, nN, E, t, v, e)) {
     flag(st, EMG_ST_INDEX, i);
     for (int k = 0; k < 64; ++k) {
       my_keys[k] = ~0ull;
@@ -66,73 +156,15 @@ __global__ void __launch_bounds__(128)
     }
     return;
   }
-  double X[3][3];
-  for (int d = 0; d < 3; ++d)
-    for (int k = 0; k < 3; ++k) X[d][k] = nodes[d * nN + v[k]];
-  double e1[3], e2[3], zh[3], xh[3], yh[3];
-  for (int d = 0; d < 3; ++d) {
-    e1[d] = X[d][1] - X[d][0];
-    e2[d] = X[d][2] - X[d][0];
-  }
-  zh[0] = e1[1] * e2[2] - e1[2] * e2[1];
-  zh[1] = e1[2] * e2[0] - e1[0] * e2[2];
-  zh[2] = e1[0] * e2[1] - e1[1] * e2[0];
-  const double nz = sqrt(zh[0] * zh[0] + zh[1] * zh[1] + zh[2] * zh[2]);
-  const double nx = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
-  for (int d = 0; d < 3; ++d) {
-    zh[d] /= nz;
-    xh[d] = e1[d] / nx;
-  }
-  yh[0] = zh[1] * xh[2] - zh[2] * xh[1];
-  yh[1] = zh[2] * xh[0] - zh[0] * xh[2];
-  yh[2] = zh[0] * xh[1] - zh[1] * xh[0];
-  const double ny = sqrt(yh[0] * yh[0] + yh[1] * yh[1] + yh[2] * yh[2]);
-  for (int d = 0; d < 3; ++d) yh[d] /= ny;
-  double tx[3], ty[3];
-  for (int k = 0; k < 3; ++k) {
-    double rx = 0.0, ry = 0.0;
-    for (int d = 0; d < 3; ++d) {
-      const double r = X[d][k] - X[d][0];
-      rx += xh[d] * r;
-      ry += yh[d] * r;
-    }
-    tx[k] = rx;
-    ty[k] = ry;
-  }
-  const double ca0 = tx[1] * ty[2] - ty[1] * tx[2], ca1 = tx[2] * ty[0] - ty[2] * tx[0],
-               ca2 = tx[0] * ty[1] - ty[0] * tx[1];
-  const double cb0 = ty[1] - ty[2], cb1 = ty[2] - ty[0], cb2 = ty[0] - ty[1];
-  const double cc0 = tx[2] - tx[1], cc1 = tx[0] - tx[2], cc2 = tx[1] - tx[0];
-  const double sA = 0.5 * (cb0 * cc1 - cb1 * cc0);
-  const double s2 = 2 * sA;
-  const double ca[3] = {ca0 / s2, ca1 / s2, ca2 / s2}, cb[3] = {cb0 / s2, cb1 / s2, cb2 / s2},
-               cc[3] = {cc0 / s2, cc1 / s2, cc2 / s2};
-  const double area = fabs(sA);
+  TriFrame T;
+  const double area = tri_frame(nodes, nN, v, T);
   if (!(area > 0.0) || !isfinite(area)) flag(st, EMG_ST_DEGENERATE, i);
   double B[36];
   for (int k = 0; k < 36; ++k) B[k] = 0.0;
 #pragma unroll 1
   for (int q = 0; q < 6; ++q) {
-    const double xs = tx[0] * kTL[0][q] + tx[1] * kTL[1][q] + tx[2] * kTL[2][q];
-    const double ys = ty[0] * kTL[0][q] + ty[1] * kTL[1][q] + ty[2] * kTL[2][q];
-    double L[3];
-    for (int m = 0; m < 3; ++m) L[m] = ca[m] + cb[m] * xs + cc[m] * ys;
     double f[8][2];
-    const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int a = EI[k], b = EJ[k];
-      const double wx = L[a] * cb[b] - L[b] * cb[a], wy = L[a] * cc[b] - L[b] * cc[a];
-      f[k][0] = wx;
-      f[k][1] = wy;
-      const double s = L[a] - L[b];
-      f[3 + k][0] = s * wx;
-      f[3 + k][1] = s * wy;
-    }
-    f[6][0] = L[0] * (L[1] * cb[2] - L[2] * cb[1]);
-    f[6][1] = L[0] * (L[1] * cc[2] - L[2] * cc[1]);
-    f[7][0] = L[1] * (L[0] * cb[2] - L[2] * cb[0]);
-    f[7][1] = L[1] * (L[0] * cc[2] - L[2] * cc[0]);
+    tri_functions(T, q, f);
     const double w = kTW[q];
     int k = 0;
 #pragma unroll
@@ -140,14 +172,8 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
       for (int b = a; b < 8; ++b, ++k) B[k] += (f[a][0] * f[b][0] + f[a][1] * f[b][1]) * w;
   }
-  // DoFs of the triangle (nedelec2.py:69-79): edges, edges + E, tri + 2E, tri + 2E + F
   int64_t dof[8];
-  for (int k = 0; k < 3; ++k) {
-    dof[k] = e[k];
-    dof[3 + k] = e[k] + E;
-  }
-  dof[6] = 2 * E + t;
-  dof[7] = 2 * E + F + t;
+  tri_dofs(e, t, E, F, dof);
   int k = 0;
   for (int a = 0; a < 8; ++a)
     for (int b = a; b < 8; ++b, ++k) {
@@ -162,6 +188,58 @@ __global__ void __launch_bounds__(128)
         my_vals[slot] = make_double2(val, 0.0);
       }
     }
+}
+
+// Port forcing vector (ned2_tri_force, robinbc.py:220-277): per boundary
+// triangle b_a = -A sum_q w_q f_a(q) . (U projected on the triangle's plane),
+// U complex [3][6][nb] at the points of generate_points_3d (:104-135); one
+// key (DoF << 32 | slot) and value per (triangle, DoF).
+__global__ void __launch_bounds__(128)
+    k_robin_force(const double *nodes, int64_t nN, const int32_t *tris, const int32_t *tri_to_edge, int64_t F,
+                  int64_t E, const int32_t *btris, int64_t nb, const double2 *U, uint64_t *keys, double2 *vals,
+                  int64_t *st) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const int64_t t = btris[i];
+  int32_t v[3], e[3];
+  if (!tri_load(tris, tri_to_edge, F, nN, E, t, v, e)) {
+    flag(st, EMG_ST_INDEX, i);
+    for (int k = 0; k < 8; ++k) {
+      keys[i * 8 + k] = ~0ull;
+      vals[i * 8 + k] = make_double2(0.0, 0.0);
+    }
+    return;
+  }
+  TriFrame T;
+  const double area = tri_frame(nodes, nN, v, T);
+  if (!(area > 0.0) || !isfinite(area)) flag(st, EMG_ST_DEGENERATE, i);
+  double br[8], bi[8];
+  for (int k = 0; k < 8; ++k) br[k] = bi[k] = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    double f[8][2];
+    tri_functions(T, q, f);
+    double ux_r = 0.0, ux_i = 0.0, uy_r = 0.0, uy_i = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double2 u = U[(d * 6 + q) * nb + i];
+      ux_r += T.xh[d] * u.x;
+      ux_i += T.xh[d] * u.y;
+      uy_r += T.yh[d] * u.x;
+      uy_i += T.yh[d] * u.y;
+    }
+    const double w = kTW[q];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      br[k] += w * (f[k][0] * ux_r + f[k][1] * uy_r);
+      bi[k] += w * (f[k][0] * ux_i + f[k][1] * uy_i);
+    }
+  }
+  int64_t dof[8];
+  tri_dofs(e, t, E, F, dof);
+  for (int k = 0; k < 8; ++k) {
+    keys[i * 8 + k] = ((uint64_t)dof[k] << 32) | (uint64_t)(i * 8 + k);
+    vals[i * 8 + k] = make_double2(-area * br[k], -area * bi[k]);
+  }
 }
 
 __global__ void k_pad_keys(uint64_t *keys, int64_t from, int64_t n_keys) {
@@ -212,6 +290,10 @@ int emg_robin_init(int64_t n_btris, emg_robin *r) {
   r->n_keys = n_btris > 0 ? pow2_at_least(r->n_slots) : 0;
   r->keys_bytes = (size_t)r->n_keys * 8;
   r->values_bytes = (size_t)r->n_slots * 16;
+  r->n_fslots = n_btris * 8;
+  r->n_fkeys = n_btris > 0 ? pow2_at_least(r->n_fslots) : 0;
+  r->fkeys_bytes = (size_t)r->n_fkeys * 8;
+  r->fvalues_bytes = (size_t)r->n_fslots * 16;
   return EMG_OK;
 }
 
@@ -245,6 +327,33 @@ int emg_robin_apply(const emg_robin *r, const uint64_t *d_keys, const void *d_va
   k_robin_apply<<<grid_for(r->n_slots, 256), 256, 0, S(stream)>>>(
       d_keys, r->n_slots, static_cast<const double2 *>(d_values), gamma_re, gamma_im, static_cast<double2 *>(d_A),
       nnz);
+  return launch_check("k_robin_apply");
+}
+
+int emg_robin_force(const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                    const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                    const void *d_U, uint64_t *d_fkeys, void *d_fvalues, void *d_b, int64_t N, int64_t *d_status,
+                    emg_stream_t stream) {
+  if (!r) return fail(EMG_EINVAL, "null robin descriptor");
+  if (r->n_btris == 0) return EMG_OK;
+  if (!d_nodes || !d_tris || !d_tri_to_edge || !d_btris || !d_U || !d_fkeys || !d_fvalues || !d_b)
+    return fail(EMG_EINVAL, "null pointer");
+  if (n_nodes <= 0 || n_tris <= 0 || n_edges <= 0 || N != 2 * n_edges + 2 * n_tris)
+    return fail(EMG_EINVAL, "bad sizes (N must be 2 E + 2 F)");
+  cudaStream_t s = S(stream);
+  k_robin_force<<<grid_for(r->n_btris, 128), 128, 0, s>>>(d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges,
+                                                          d_btris, r->n_btris, static_cast<const double2 *>(d_U),
+                                                          d_fkeys, static_cast<double2 *>(d_fvalues), d_status);
+  int rc = launch_check("k_robin_force");
+  if (rc) return rc;
+  if (r->n_fkeys > r->n_fslots) {
+    k_pad_keys<<<grid_for(r->n_fkeys - r->n_fslots, 256), 256, 0, s>>>(d_fkeys, r->n_fslots, r->n_fkeys);
+    if ((rc = launch_check("k_pad_keys"))) return rc;
+  }
+  if ((rc = sort_u64(d_fkeys, r->n_fkeys, s))) return rc;
+  k_robin_apply<<<grid_for(r->n_fslots, 256), 256, 0, s>>>(d_fkeys, r->n_fslots,
+                                                           static_cast<const double2 *>(d_fvalues), 1.0, 0.0,
+                                                           static_cast<double2 *>(d_b), N);
   return launch_check("k_robin_apply");
 }
 

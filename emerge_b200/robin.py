@@ -30,6 +30,15 @@ from .assembly import GpuCSCMapping, LinComb, _to_dev
 
 __all__ = ["RobinTerm", "assemble_robin_bc"]
 
+# barycentric rows L1..L3 of the 6-point triangle rule (robinbc.py:189-196)
+_TRI_L = np.array([
+    [0.81684757298045896, 0.09157621350977101, 0.09157621350977101, 0.10810301816807000, 0.44594849091596500,
+     0.44594849091596500],
+    [0.09157621350977101, 0.81684757298045896, 0.09157621350977101, 0.44594849091596500, 0.10810301816807000,
+     0.44594849091596500],
+    [0.09157621350977004, 0.09157621350977008, 0.81684757298045807, 0.44594849091596500, 0.44594849091596500,
+     0.10810301816807000]])
+
 
 class RobinTerm:
     """The boundary term of the triangles ``tri_ids`` (int, into
@@ -54,23 +63,65 @@ class RobinTerm:
         self.desc = r
         self.d_keys = torch.empty(max(r.n_keys, 1), dtype=torch.int64, device=dev)
         self.d_vals = torch.empty(max(r.n_slots, 1), dtype=torch.complex128, device=dev)
+        self._field, self._ids = field, ids
         if self.n_btris:
-            nodes = _to_dev(m.nodes, torch.float64, dev)
-            tris = _to_dev(m.tris, torch.int32, dev)
-            t2e = _to_dev(m.tri_to_edge, torch.int32, dev)
-            btris = _to_dev(ids, torch.int32, dev)
-            status = torch.zeros(2, dtype=torch.int64, device=dev)
-            st = L.stream_handle(dev)
-            L.check(L.lib().emg_robin_build(L.ctypes.byref(r), L.ptr(nodes), m.n_nodes, L.ptr(tris), L.ptr(t2e),
-                                            m.n_tris, m.n_edges, L.ptr(btris), L.ptr(cscmap.d_indptr),
-                                            L.ptr(cscmap.d_indices), cscmap.N, L.ptr(self.d_keys),
-                                            L.ptr(self.d_vals), L.ptr(status), st))
-            f, i = L.ctypes.c_int64(), L.ctypes.c_int64()
-            L.check(L.lib().emg_status_read(L.ptr(status), L.ctypes.byref(f), L.ctypes.byref(i), st))
-            if f.value:
-                raise L.EmgMeshError(L.EMG_EMESH, f"boundary triangle {int(ids[i.value]) if 0 <= i.value < ids.size else i.value}: "
-                                     + ("outside the assembled pattern or bad index" if f.value & L.EMG_ST_INDEX
-                                        else "degenerate triangle"))
+            self._nodes = _to_dev(m.nodes, torch.float64, dev)
+            self._tris = _to_dev(m.tris, torch.int32, dev)
+            self._t2e = _to_dev(m.tri_to_edge, torch.int32, dev)
+            self._btris = _to_dev(ids, torch.int32, dev)
+            self._status = torch.zeros(2, dtype=torch.int64, device=dev)
+            L.check(L.lib().emg_robin_build(L.ctypes.byref(r), L.ptr(self._nodes), m.n_nodes, L.ptr(self._tris),
+                                            L.ptr(self._t2e), m.n_tris, m.n_edges, L.ptr(self._btris),
+                                            L.ptr(cscmap.d_indptr), L.ptr(cscmap.d_indices), cscmap.N,
+                                            L.ptr(self.d_keys), L.ptr(self.d_vals), L.ptr(self._status),
+                                            L.stream_handle(dev)))
+            self._check("outside the assembled pattern or bad index")
+
+    def _check(self, what: str) -> None:
+        st = L.stream_handle(self.cmap.device)
+        f, i = L.ctypes.c_int64(), L.ctypes.c_int64()
+        L.check(L.lib().emg_status_read(L.ptr(self._status), L.ctypes.byref(f), L.ctypes.byref(i), st))
+        if f.value:
+            t = int(self._ids[i.value]) if 0 <= i.value < self._ids.size else i.value
+            raise L.EmgMeshError(L.EMG_EMESH, f"boundary triangle {t}: "
+                                 + (what if f.value & L.EMG_ST_INDEX else "degenerate triangle"))
+
+    def quadrature_points(self) -> np.ndarray:
+        """The 6 quadrature points of every listed triangle, f8[3, 6, n_btris]
+        (generate_points_3d, robinbc.py:104-135): where the caller evaluates
+        the incident field for ``force``."""
+        m = self._field.mesh
+        v = m.nodes[:, m.tris[:, self._ids]]  # (3, 3 vertices, nb)
+        return np.einsum("dvn,vq->dqn", v, _TRI_L)
+
+    def force(self, U, b: torch.Tensor | None = None) -> torch.Tensor:
+        """Port forcing vector (assemble_robin_bc_bvec, robinbc.py:405-433):
+        b (complex128 [N], device) += the triangles' entries for the incident
+        field U (complex [3, 6, n_btris] at ``quadrature_points``)."""
+        dev = self.cmap.device
+        if b is None:
+            b = torch.zeros(self.cmap.N, dtype=torch.complex128, device=dev)
+        if b.dtype != torch.complex128 or b.numel() != self.cmap.N:
+            raise ValueError("b must be complex128 with N values")
+        if not self.n_btris:
+            return b
+        if isinstance(U, torch.Tensor):
+            Ud = U.to(device=dev, dtype=torch.complex128).contiguous()
+        else:
+            Ud = _to_dev(np.asarray(U, dtype=np.complex128), torch.complex128, dev)
+        if tuple(Ud.shape) != (3, 6, self.n_btris):
+            raise ValueError(f"U must have shape (3, 6, {self.n_btris})")
+        r = self.desc
+        fkeys = torch.empty(max(r.n_fkeys, 1), dtype=torch.int64, device=dev)
+        fvals = torch.empty(max(r.n_fslots, 1), dtype=torch.complex128, device=dev)
+        m = self._field.mesh
+        self._status.zero_()
+        L.check(L.lib().emg_robin_force(L.ctypes.byref(r), L.ptr(self._nodes), m.n_nodes, L.ptr(self._tris),
+                                        L.ptr(self._t2e), m.n_tris, m.n_edges, L.ptr(self._btris), L.ptr(Ud),
+                                        L.ptr(fkeys), L.ptr(fvals), L.ptr(b), self.cmap.N, L.ptr(self._status),
+                                        L.stream_handle(dev)))
+        self._check("bad index")
+        return b
 
     def _lc(self) -> LinComb:
         return LinComb(None, {self: 1.0 + 0.0j})

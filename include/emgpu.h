@@ -258,6 +258,10 @@ typedef struct {
   int64_t n_keys;      /* power of two >= n_slots: length of the sorted key array */
   size_t keys_bytes;   /* 8 * n_keys: d_keys of build/apply */
   size_t values_bytes; /* 16 * n_slots: d_values (complex128) of build/apply */
+  int64_t n_fslots;    /* 8 per triangle: its forcing-vector entries */
+  int64_t n_fkeys;     /* power of two >= n_fslots */
+  size_t fkeys_bytes;  /* 8 * n_fkeys: d_fkeys of emg_robin_force */
+  size_t fvalues_bytes; /* 16 * n_fslots: d_fvalues of emg_robin_force */
 } emg_robin;
 
 /* Host-only: sizes for n_btris triangles (fewer than 2^26). */
@@ -280,6 +284,17 @@ int emg_robin_build(const emg_robin *robin, const double *d_nodes, int64_t n_nod
  * values of A (complex128); stream-ordered, deterministic. */
 int emg_robin_apply(const emg_robin *robin, const uint64_t *d_keys, const void *d_values, double gamma_re,
                     double gamma_im, void *d_A, int64_t nnz, emg_stream_t stream);
+
+/* Port forcing vector: d_b[N] (complex128) += the boundary triangles'
+ * ned2_tri_force entries (robinbc.py:220-313, assemble_robin_bc_bvec
+ * :405-433) for the incident field d_U (complex128 [3][6][n_btris]: component,
+ * quadrature point of the 6-point rule, triangle; the points are those of
+ * generate_points_3d :104-135). Each DoF sums its triangles in list order.
+ * Scratch d_fkeys / d_fvalues: robin->fkeys_bytes / fvalues_bytes. */
+int emg_robin_force(const emg_robin *robin, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                    const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                    const void *d_U, uint64_t *d_fkeys, void *d_fvalues, void *d_b, int64_t N, int64_t *d_status,
+                    emg_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -10,6 +10,9 @@ surface on numpy arrays:
 * ``tri_stiff``, ``robin_entries``, ``tri_rowcol``, ``generate_csc``
                        -> robinbc.py:316-402 (``ned2_tri_stiff``,
                           ``compute_bc_entries``), femdata.py:52-56,75-92,104-118
+* ``tri_force``, ``force_entries``, ``tri_points`` -> robinbc.py:104-135,220-313
+                          (``generate_points_3d``, ``ned2_tri_force``,
+                          ``compute_force_entries``)
 * ``topology_loops``   -> mesh3d.py:706-776 and nedelec2.py:61-79 restated as
   plain Python loops (small meshes only; checks the vectorised host topology)
 
@@ -66,6 +69,10 @@ def lib():
         L.oracle_tri_stiff.argtypes = [_p, ctypes.c_double, ctypes.c_double, _p]
         L.oracle_robin_entries.restype = ctypes.c_int
         L.oracle_robin_entries.argtypes = [_p, _i64, _p, _i64, _p, _i64, ctypes.c_double, ctypes.c_double, _p]
+        L.oracle_tri_force.restype = None
+        L.oracle_tri_force.argtypes = [_p, _p, _p]
+        L.oracle_force_entries.restype = ctypes.c_int
+        L.oracle_force_entries.argtypes = [_p, _i64, _p, _i64, _p, _p, _i64, _p, _i64, _p]
         _lib = L
     return _lib
 
@@ -243,3 +250,55 @@ def generate_csc(field, data: np.ndarray) -> csc_matrix:
     rows, cols = tri_rowcol(field)
     ids = np.argwhere(data != 0)[:, 0]
     return csc_matrix((data[ids], (rows[ids], cols[ids])), shape=(field.n_field, field.n_field))
+
+
+def tri_force(X: np.ndarray, U: np.ndarray) -> np.ndarray:
+    """``ned2_tri_force`` (robinbc.py:220-277): X f8[3, 3] vertex coordinates,
+    U c16[3, 6] the incident field at the 6 points -> c16[8]."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    out = np.empty(8, np.complex128)
+    lib().oracle_tri_force(_ptr(X), _ptr(U), _ptr(out))
+    return out
+
+
+def tri_points(field, tri_ids) -> np.ndarray:
+    """``generate_points_3d`` (robinbc.py:104-135) as loops: the 6 quadrature
+    points of every listed tri, f8[3, 6, nb]."""
+    m = field.mesh
+    D = np.array([[0.81684757298045896, 0.09157621350977101, 0.09157621350977101, 0.10810301816807000,
+                   0.44594849091596500, 0.44594849091596500],
+                  [0.09157621350977101, 0.81684757298045896, 0.09157621350977101, 0.44594849091596500,
+                   0.10810301816807000, 0.44594849091596500],
+                  [0.09157621350977004, 0.09157621350977008, 0.81684757298045807, 0.44594849091596500,
+                   0.44594849091596500, 0.10810301816807000]])
+    ids = np.asarray(tri_ids, dtype=np.int64)
+    out = np.empty((3, 6, ids.size))
+    for i, t in enumerate(ids):
+        v = m.tris[:, t]
+        for d in range(3):
+            x1, x2, x3 = m.nodes[d, v]
+            out[d, :, i] = x1 * D[0] + x2 * D[1] + x3 * D[2]
+    return out
+
+
+def force_entries(field, tri_ids, U: np.ndarray, b: np.ndarray | None = None) -> np.ndarray:
+    """``assemble_robin_bc_bvec`` / ``compute_force_entries`` (robinbc.py:280-313,
+    405-433): b[tri_to_field[:, t]] += ned2_tri_force(t) for every listed tri,
+    U c16[3, 6, nb] the incident field at ``tri_points``."""
+    m = field.mesh
+    N = int(field.n_field)
+    if b is None:
+        b = np.zeros(N, np.complex128)
+    ids = np.ascontiguousarray(tri_ids, dtype=np.int64)
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    if U.shape != (3, 6, ids.size):
+        raise ValueError("U must have shape (3, 6, n_tris)")
+    nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+    tris = np.ascontiguousarray(m.tris, dtype=np.int64)
+    t2f = np.ascontiguousarray(field.tri_to_field, dtype=np.int64)
+    rc = lib().oracle_force_entries(_ptr(nodes), nodes.shape[1], _ptr(tris), tris.shape[1], _ptr(t2f), _ptr(ids),
+                                    ids.size, _ptr(U), N, _ptr(b))
+    if rc != 0:
+        raise IndexError("tri id or index out of range")
+    return b

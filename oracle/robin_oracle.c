@@ -9,6 +9,7 @@
  *   tri_coefficients                             robinbc.py:200-221
  *   DPTS (6-point triangle rule)                 robinbc.py:189-196
  *   compute_bc_entries                           robinbc.py:381-402
+ *   ned2_tri_force / compute_force_entries       robinbc.py:220-313
  *   2-D basis functions _ne0_2d, _ne2_2d, _nf0_2d, _nf1_2d
  *                                                compiled/ccbf.py:81,107,269,284
  *
@@ -51,8 +52,11 @@ static void normalize3(double a[3]) {
   a[2] /= n;
 }
 
-/* X[d][v]: vertex v (0..2) coordinates. out[64] row-major, gamma applied. */
-void oracle_tri_stiff(const double X[3][3], double g_re, double g_im, cplx *out) {
+/* The triangle's local frame (construct_local_vertices), coefficients
+ * (tri_coefficients) and the 8 Volakis functions at the 6 points.
+ * X[d][v]: vertex v (0..2) coordinates. Returns the area; basis rows are
+ * xhat, yhat, zhat. */
+static double tri_frame_basis(const double X[3][3], double basis[3][3], double f[8][2][6]) {
   /* construct_local_vertices: origin at vertex 0, x along edge 0->1, z the normal */
   double e1[3], e2[3], xh[3], yh[3], zh[3];
   for (int d = 0; d < 3; ++d) {
@@ -65,6 +69,11 @@ void oracle_tri_stiff(const double X[3][3], double g_re, double g_im, cplx *out)
   normalize3(xh);
   cross3(zh, xh, yh);
   normalize3(yh);
+  for (int d = 0; d < 3; ++d) {
+    basis[0][d] = xh[d];
+    basis[1][d] = yh[d];
+    basis[2][d] = zh[d];
+  }
   double tx[3], ty[3];
   for (int v = 0; v < 3; ++v) {
     double rx = 0.0, ry = 0.0;
@@ -88,10 +97,8 @@ void oracle_tri_stiff(const double X[3][3], double g_re, double g_im, cplx *out)
     cb[m] = b[m] / (2 * sA);
     cc[m] = c[m] / (2 * sA);
   }
-  const double area = fabs(sA);
   /* the 8 basis functions at the 6 points */
   static const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
-  double f[8][2][6];
   for (int q = 0; q < 6; ++q) {
     const double xs = tx[0] * TRI_DPTS[1][q] + tx[1] * TRI_DPTS[2][q] + tx[2] * TRI_DPTS[3][q];
     const double ys = ty[0] * TRI_DPTS[1][q] + ty[1] * TRI_DPTS[2][q] + ty[2] * TRI_DPTS[3][q];
@@ -113,6 +120,13 @@ void oracle_tri_stiff(const double X[3][3], double g_re, double g_im, cplx *out)
     f[7][0][q] = L[1] * (L[0] * cb[2] - L[2] * cb[0]);
     f[7][1][q] = L[1] * (L[0] * cc[2] - L[2] * cc[0]);
   }
+  return fabs(sA);
+}
+
+/* X[d][v]: vertex v (0..2) coordinates. out[64] row-major, gamma applied. */
+void oracle_tri_stiff(const double X[3][3], double g_re, double g_im, cplx *out) {
+  double basis[3][3], f[8][2][6];
+  const double area = tri_frame_basis(X, basis, f);
   const cplx g = g_re + I * g_im;
   for (int p = 0; p < 8; ++p)
     for (int r = 0; r < 8; ++r) {
@@ -140,6 +154,50 @@ int oracle_robin_entries(const double *nodes, int64_t nN, const int64_t *tris, i
     cplx B[64];
     oracle_tri_stiff(X, g_re, g_im, B);
     for (int k = 0; k < 64; ++k) Bmat[t * 64 + k] += B[k];
+  }
+  return 0;
+}
+
+/* ned2_tri_force: out[8] = -A sum_q w_q f_a(q) . U2(q), with U2 the first two
+ * components of the incident field in the triangle's frame (basis @ U).
+ * U: complex [3][6] (component, point). */
+void oracle_tri_force(const double X[3][3], const cplx *U, cplx *out) {
+  double basis[3][3], f[8][2][6];
+  const double area = tri_frame_basis(X, basis, f);
+  cplx u2[2][6];
+  for (int a = 0; a < 2; ++a)
+    for (int q = 0; q < 6; ++q) u2[a][q] = basis[a][0] * U[0 * 6 + q] + basis[a][1] * U[1 * 6 + q] + basis[a][2] * U[2 * 6 + q];
+  for (int p = 0; p < 8; ++p) {
+    cplx sum = 0.0;
+    for (int q = 0; q < 6; ++q) sum += TRI_DPTS[0][q] * (f[p][0][q] * u2[0][q] + f[p][1][q] * u2[1][q]);
+    out[p] = -area * sum;
+  }
+}
+
+/* compute_force_entries: b[tri_to_field[:, itri]] += force(itri) for every
+ * listed tri, U: complex [3][6][nb] (the reference's U_global_all layout),
+ * t2f: int64 [8][F]. */
+int oracle_force_entries(const double *nodes, int64_t nN, const int64_t *tris, int64_t F, const int64_t *t2f,
+                         const int64_t *btris, int64_t nb, const cplx *U, int64_t N, cplx *b) {
+  for (int64_t i = 0; i < nb; ++i) {
+    const int64_t t = btris[i];
+    if (t < 0 || t >= F) return -1;
+    for (int v = 0; v < 3; ++v)
+      if (tris[v * F + t] < 0 || tris[v * F + t] >= nN) return -1;
+    for (int k = 0; k < 8; ++k)
+      if (t2f[k * F + t] < 0 || t2f[k * F + t] >= N) return -1;
+  }
+  for (int64_t i = 0; i < nb; ++i) {
+    const int64_t t = btris[i];
+    double X[3][3];
+    for (int d = 0; d < 3; ++d)
+      for (int v = 0; v < 3; ++v) X[d][v] = nodes[d * nN + tris[v * F + t]];
+    cplx Ui[18];
+    for (int d = 0; d < 3; ++d)
+      for (int q = 0; q < 6; ++q) Ui[d * 6 + q] = U[(d * 6 + q) * nb + i];
+    cplx bv[8];
+    oracle_tri_force(X, Ui, bv);
+    for (int k = 0; k < 8; ++k) b[t2f[k * F + t]] += bv[k];
   }
   return 0;
 }

@@ -10,7 +10,12 @@ Writes tests/golden/robin.npz:
   mixed scales, offsets and orientations, complex gamma;
 * port_ids (nb,), port_gamma, port_B (nb, 64): compute_bc_entries over the
   two port faces (z = 0 and z = 50 mm) of the 12x6x30 WR-90 air box at 10 GHz
-  with the TE10 gamma = j beta (port_bcs.py:963-983).
+  with the TE10 gamma = j beta (port_bcs.py:963-983);
+* tri_U (16, 3, 6), tri_f (16, 8): ned2_tri_force (:220-277) of the same
+  single triangles with random complex fields;
+* port_pts (3, 6, nb) from generate_points_3d (:104-135) and port_b (N,):
+  compute_force_entries (:280-313) over the port faces with the field
+  U = (0, (1 + 0.5j) sin(pi x / a), 0).
 """
 import os
 import sys
@@ -47,8 +52,21 @@ def main():
     Bmat = R.robinbc.compute_bc_entries(np.ascontiguousarray(m.nodes), np.ascontiguousarray(m.tris), Bmat, ids,
                                         complex(gamma), DOFCODES_2D)
     port_B = Bmat.reshape(m.n_tris, 64)[ids]
+    Us = [rng.normal(size=(3, 6)) + 1j * rng.normal(size=(3, 6)) for _ in Xs]
+    fs = [np.asarray(R.robinbc.ned2_tri_force(np.ascontiguousarray(X), np.ascontiguousarray(U), DOFCODES_2D))
+          for X, U in zip(Xs, Us)]
+    D = np.ascontiguousarray(R.robinbc.DPTS)
+    xf, yf, zf = R.robinbc.generate_points_3d(np.ascontiguousarray(m.nodes), np.ascontiguousarray(m.tris), D, ids)
+    pts = np.stack([xf, yf, zf]).reshape(3, D.shape[1], ids.size)
+    U = np.zeros((3, D.shape[1], ids.size), np.complex128)
+    U[1] = (1 + 0.5j) * np.sin(np.pi * pts[0] / W.WR90[0])
+    tri_to_field = np.ascontiguousarray(wl.field.tri_to_field)
+    b = R.robinbc.compute_force_entries(np.ascontiguousarray(m.nodes), np.ascontiguousarray(m.tris),
+                                        np.zeros(wl.field.n_field, np.complex128), ids, U, tri_to_field,
+                                        DOFCODES_2D)
     np.savez_compressed(os.path.join(HERE, "robin.npz"), tri_X=np.array(Xs), tri_gamma=np.array(gs),
-                        tri_B=np.array(Bs), port_ids=ids, port_gamma=np.complex128(gamma), port_B=port_B)
+                        tri_B=np.array(Bs), port_ids=ids, port_gamma=np.complex128(gamma), port_B=port_B,
+                        tri_U=np.array(Us), tri_f=np.array(fs), port_pts=pts, port_b=b)
     print("tris", len(Xs), "port tris", ids.size, "gamma", gamma)
 
 

@@ -47,3 +47,24 @@ def test_robin_csc_lies_in_the_volume_pattern():
     S.sum_duplicates()
     assert S.nnz == cmap.nnz
     assert R.nnz > 0 and np.array_equal(np.sort(ids), np.unique(ids))
+
+
+def test_force_single_triangles_match_reference():
+    g = load_npz("robin.npz")
+    for X, U, fref in zip(g["tri_X"], g["tri_U"], g["tri_f"]):
+        mine = O.tri_force(X, U)
+        assert np.abs(mine - fref).max() <= TOL * np.abs(fref).max()
+
+
+def test_force_on_port_faces_matches_reference():
+    g = load_npz("robin.npz")
+    wl = W.wr90_air()
+    ids = g["port_ids"]
+    pts = O.tri_points(wl.field, ids)
+    assert np.abs(pts - g["port_pts"]).max() <= 1e-15 * np.abs(pts).max()
+    U = np.zeros(pts.shape, np.complex128)
+    U[1] = (1 + 0.5j) * np.sin(np.pi * g["port_pts"][0] / W.WR90[0])
+    b = O.force_entries(wl.field, ids, U)
+    ref = g["port_b"]
+    assert np.abs(b - ref).max() <= TOL * np.abs(ref).max()
+    assert np.count_nonzero(ref) > 0
