@@ -47,6 +47,8 @@ def parse():
                     help="resident frequency sweep: 201 frequencies 8-12 GHz with the two port terms on the workload")
     ap.add_argument("--sweep-freqs", type=int, default=201)
     ap.add_argument("--sweep-batch", type=int, default=8, help="frequencies formed per launch (outputs resident)")
+    ap.add_argument("--pml", action="store_true",
+                    help="anisotropic PML shell + 2%% slivers (1,008,000 tets): speed and mixed-vs-FP64 errors")
     ap.add_argument("--shard", action="store_true",
                     help="strong scaling: one assembly column-sharded over the ranks instead of one replica per rank")
     ap.add_argument("--serving", action="store_true",
@@ -439,6 +441,78 @@ def run_sweep(args, rank, world, local_rank):
             "clocks": sampler.summary(), "gpu_launches": args.steps * (n_launch + 2 * nf)}
 
 
+def run_pml(args, rank, world, local_rank):
+    """--pml: the 84x50x40 PML + slivers workload (diagonal complex er = ur in
+    the outer 10% shell, 2% slivers): assembly speed of both forms and the
+    mixed form's relative error against FP64 for K, M, A, also with only one
+    diagonal tensor component kept (the others 1), on the device."""
+    import torch
+
+    from emerge_b200 import _lib as L
+    from emerge_b200 import workloads as W
+    from emerge_b200.assembly import DeviceMaterial, DeviceMesh, GpuCSCMapping, _Job
+    from emerge_b200.ranks import max_over_ranks
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = W.wr90_pml_slivers()
+    f = wl.field
+    dm = DeviceMesh(f, wl.conductor_tets, dev)
+    cmap = GpuCSCMapping(dm)
+    k0 = wl.k0
+    alpha, beta = 1.0 + 0j, complex(-k0 ** 2)
+    stream = torch.cuda.current_stream(dev)
+    dmat = DeviceMaterial(wl.er, wl.ur, f.ntets, dev)
+    out = torch.empty(cmap.nnz, dtype=torch.complex128, device=dev)
+    times = {}
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        for name, prec in (("fp64", L.EMG_FP64), ("mixed", L.EMG_MIXED)):
+            job = _Job(dm, dmat, prec)
+            times[name] = time_steps(lambda: cmap.assemble_device(job, alpha, beta, out), args.steps, args.warmup,
+                                     stream)
+    dm.check_status()
+    times = dict(zip(times, max_over_ranks(list(times.values()), dev)))
+
+    def comp(t, c):
+        o = np.zeros_like(t)
+        for d in range(3):
+            o[d, d] = t[d, d] if d == c else 1.0
+        return o
+
+    def rel(a, b):
+        d = (a - b).abs()
+        return {"fro": float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)),
+                "max": float(d.max() / b.abs().max())}
+
+    errors = {}
+    for cname, c in (("xx", 0), ("yy", 1), ("zz", 2), ("full", None)):
+        er = wl.er if c is None else comp(wl.er, c)
+        ur = wl.ur if c is None else comp(wl.ur, c)
+        mat = DeviceMaterial(er, ur, f.ntets, dev)
+        res = {}
+        for key, a, b in (("K", 1.0 + 0j, 0j), ("M", 0j, 1.0 + 0j), ("A", alpha, beta)):
+            v64 = cmap.assemble_device(_Job(dm, mat, L.EMG_FP64), a, b).clone()
+            v32 = cmap.assemble_device(_Job(dm, mat, L.EMG_MIXED), a, b)
+            res[key] = rel(v32[: cmap.nnz], v64[: cmap.nnz])
+            del v64, v32
+        errors[cname] = res
+    dm.check_status()
+    if rank != 0:
+        return None
+    nT, nnz, nN = f.ntets, cmap.nnz, f.mesh.n_nodes
+    balg = W.alg_bytes(nN, nT, nnz, 96)
+    return {"metric": "tets/s assembled, anisotropic PML + slivers workload (mixed form; FP64 beside)",
+            "value": world * nT / (times["mixed"] * 1e-3), "unit": "tets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": times["mixed"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "mixed", "data": "synthetic",
+            "config": {"workload": wl.name, "tets": nT, "hex_grid": list(wl.hex_grid), "nnz": nnz,
+                       "slivers": int(len(wl.slivers)), "material": "diagonal complex er = ur (PML shell)",
+                       "alg_bytes_per_step": balg},
+            "plain_fp64": {"value": world * nT / (times["fp64"] * 1e-3), "ms_per_step": times["fp64"]},
+            "mixed_vs_fp64_errors": errors, "clocks": sampler.summary(), "gpu_launches": 4 * args.steps}
+
+
 def run_shard(args, rank, world, local_rank):
     """--shard: the workload's columns split over the ranks (each rank
     assembles the tets touching its edges/faces, no exchange step); one step
@@ -541,6 +615,8 @@ def main():
         line, wl = run_shard(args, rank, world, local_rank), None
     elif args.sweep:
         line, wl = run_sweep(args, rank, world, local_rank), None
+    elif args.pml:
+        line, wl = run_pml(args, rank, world, local_rank), None
     else:
         line, wl = run_ours(args, rank, world, local_rank)
     if rank == 0 and not args.no_cpu_baseline and wl is not None:

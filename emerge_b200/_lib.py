@@ -25,6 +25,7 @@ EXPORTS = (
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
     "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
+    "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values",
 )
 
 
@@ -56,6 +57,11 @@ class Robin(ctypes.Structure):
     _fields_ = [("n_btris", ctypes.c_int64), ("n_slots", ctypes.c_int64), ("n_keys", ctypes.c_int64),
                 ("keys_bytes", ctypes.c_size_t), ("values_bytes", ctypes.c_size_t), ("n_fslots", ctypes.c_int64),
                 ("n_fkeys", ctypes.c_int64), ("fkeys_bytes", ctypes.c_size_t), ("fvalues_bytes", ctypes.c_size_t)]
+
+
+class Select(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int64), ("M", ctypes.c_int64), ("nnz_sel", ctypes.c_int64),
+                ("workspace_bytes", ctypes.c_size_t)]
 
 
 class FormItem(ctypes.Structure):
@@ -108,6 +114,10 @@ def lib():
     L.emg_robin_build.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P,
                                   _P]
     L.emg_robin_apply.argtypes = [ctypes.POINTER(Robin), _P, _P, _D, _D, _P, _I64, _P]
+    L.emg_select_init.argtypes = [_I64, ctypes.POINTER(Select)]
+    L.emg_select_build.argtypes = [ctypes.POINTER(Select), _P, _P, _P, _P, _P, _P, _P]
+    L.emg_select_finish.argtypes = [ctypes.POINTER(Select), _P, _P, _P, _P, _P, _P, _P, _P]
+    L.emg_select_values.argtypes = [ctypes.POINTER(Select), _P, _P, _I64, _P, _P]
     L.emg_robin_force.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P,
                                   _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
@@ -115,7 +125,8 @@ def lib():
     for name in ("emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
                  "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_robin_init", "emg_robin_build",
-                 "emg_robin_apply", "emg_robin_force"):
+                 "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
+                 "emg_select_values"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -150,6 +150,11 @@ int plan_finish(const emg_plan *p, const int32_t *t2e, const int32_t *t2t, const
                 const int32_t *indptr, int32_t *indices, int64_t *st, cudaStream_t s);
 int plan_order(const emg_plan *p, void *d_plan, const double *nodes, int64_t nN, const int32_t *tets,
                const int32_t *tetids, void *d_ws, cudaStream_t s);
+// exclusive prefix sum of n int32 counts into out[0..n] (out[n] = total; in
+// and out may alias); bsum: scan_i32_bsum_bytes(n) of scratch
+int scan_i32(const int32_t *in, int64_t n, int32_t *out, long long *bsum, int64_t *st, cudaStream_t s);
+size_t scan_i32_bsum_bytes(int64_t n);
+
 // ascending bitonic sort of n2 (a power of two) 64-bit keys in place
 int sort_u64(uint64_t *keys, int64_t n2, cudaStream_t s);
 inline int64_t pow2_at_least(int64_t n) {

@@ -508,6 +508,11 @@ int status_reset(int64_t *st, cudaStream_t s) {
   return launch_check("k_status_reset");
 }
 
+int scan_i32(const int32_t *in, int64_t n, int32_t *out, long long *bsum, int64_t *st, cudaStream_t s) {
+  return exclusive_scan(in, n, out, bsum, st, s);
+}
+size_t scan_i32_bsum_bytes(int64_t n) { return scan_bsum_bytes(n); }
+
 size_t plan_layout(emg_plan *p) {
   size_t o = 0;
   p->off_ent_ptr = o;

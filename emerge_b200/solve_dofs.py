@@ -1,0 +1,79 @@
+"""The solve-DoF submatrix on the device.
+
+Before every solve the reference slices the assembled system to the DoFs that
+are not fixed by PEC conditions (solver.py:2071)::
+
+    Asel = A[:, solve_ids][solve_ids, :]
+    bsel = b[solve_ids]
+
+``SolveSubmatrix(cscmap, solve_ids)`` builds the reduced pattern once (rows
+renumbered and ascending, as scipy's slicing gives them) and a map from each
+kept entry to its position in A; per frequency ``values(A)`` gathers the
+reduced values on the device, so a GPU solver never needs A on the host.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+from scipy.sparse import csc_matrix
+
+from . import _lib as L
+from .assembly import GpuCSCMapping, _to_dev
+
+__all__ = ["SolveSubmatrix"]
+
+
+class SolveSubmatrix:
+    """A[:, solve_ids][solve_ids, :] of the pattern of ``cscmap``;
+    ``solve_ids`` are DoF numbers (any order, duplicates ignored)."""
+
+    def __init__(self, cscmap: GpuCSCMapping, solve_ids):
+        self.cmap = cscmap
+        dev = cscmap.device
+        N = cscmap.N
+        ids = np.unique(np.asarray(solve_ids, dtype=np.int64).ravel())
+        if ids.size and (ids[0] < 0 or ids[-1] >= N):
+            raise IndexError("solve id out of range")
+        self.solve_ids = ids
+        keep = np.zeros(N, np.uint8)
+        keep[ids] = 1
+        d_keep = _to_dev(keep, torch.uint8, dev)
+        sel = L.Select()
+        L.check(L.lib().emg_select_init(N, L.ctypes.byref(sel)))
+        ws = torch.empty(max(sel.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+        self.d_indptr = torch.empty(N + 1, dtype=torch.int32, device=dev)
+        status = torch.zeros(2, dtype=torch.int64, device=dev)
+        st = L.stream_handle(dev)
+        L.check(L.lib().emg_select_build(L.ctypes.byref(sel), L.ptr(cscmap.d_indptr), L.ptr(cscmap.d_indices),
+                                         L.ptr(d_keep), L.ptr(ws), L.ptr(self.d_indptr), L.ptr(status), st))
+        self.M, self.nnz = int(sel.M), int(sel.nnz_sel)
+        self.d_indices = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
+        self.d_take = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
+        L.check(L.lib().emg_select_finish(L.ctypes.byref(sel), L.ptr(cscmap.d_indptr), L.ptr(cscmap.d_indices),
+                                          L.ptr(d_keep), L.ptr(ws), L.ptr(self.d_indptr), L.ptr(self.d_indices),
+                                          L.ptr(self.d_take), st))
+        self.sel = sel
+        self.d_ids = _to_dev(ids, torch.int64, dev)
+
+    def values(self, A: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Asel's values (complex128 [nnz_sel], device) from A's (complex128
+        [nnz], device); stream-ordered."""
+        if A.dtype != torch.complex128 or A.numel() < self.cmap.nnz:
+            raise ValueError("A must be complex128 with nnz values")
+        if out is None:
+            out = torch.empty(max(self.nnz, 1), dtype=torch.complex128, device=self.cmap.device)
+        L.check(L.lib().emg_select_values(L.ctypes.byref(self.sel), L.ptr(self.d_take), L.ptr(A), self.cmap.nnz,
+                                          L.ptr(out), L.stream_handle(self.cmap.device)))
+        return out[: self.nnz]
+
+    def rhs(self, b: torch.Tensor) -> torch.Tensor:
+        """b[solve_ids] on the device."""
+        return b.index_select(0, self.d_ids)
+
+    def to_csc(self, data) -> csc_matrix:
+        """Asel as a host csc_matrix; data: anything ``cscmap.to_device``
+        takes (element-value combinations, boundary terms) or A's device values."""
+        A = data if isinstance(data, torch.Tensor) else self.cmap.to_device(data)
+        v = self.values(A).cpu().numpy()
+        return csc_matrix((v, self.d_indices[: self.nnz].cpu().numpy(), self.d_indptr[: self.M + 1].cpu().numpy()),
+                          shape=(self.M, self.M))

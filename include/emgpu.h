@@ -296,6 +296,30 @@ int emg_robin_force(const emg_robin *robin, const double *d_nodes, int64_t n_nod
                     const void *d_U, uint64_t *d_fkeys, void *d_fvalues, void *d_b, int64_t N, int64_t *d_status,
                     emg_stream_t stream);
 
+/* Solve-DoF submatrix: Asel = A[:, solve_ids][solve_ids, :] on the device
+ * (solver.py:2071; solve_ids = the DoFs that are not PEC, assembler.py:
+ * 543-564,742). d_keep: uint8 [N], 1 for a solve DoF. The pattern (indptr_sel
+ * [M+1], indices_sel [nnz_sel], rows renumbered and ascending as scipy's
+ * slicing gives them) and the take map (position in A of each selected
+ * entry) are built once; emg_select_values gathers the values per frequency. */
+typedef struct {
+  int64_t N;              /* columns of A */
+  int64_t M;              /* solve DoFs (set by emg_select_build) */
+  int64_t nnz_sel;        /* nonzeros of Asel (set by emg_select_build) */
+  size_t workspace_bytes; /* scratch of build and finish (keep it between them) */
+} emg_select;
+
+int emg_select_init(int64_t N, emg_select *sel);
+/* d_indptr_sel needs N + 1 entries (M + 1 are used); synchronises stream. */
+int emg_select_build(emg_select *sel, const int32_t *d_indptr, const int32_t *d_indices, const uint8_t *d_keep,
+                     void *d_workspace, int32_t *d_indptr_sel, int64_t *d_status, emg_stream_t stream);
+int emg_select_finish(const emg_select *sel, const int32_t *d_indptr, const int32_t *d_indices, const uint8_t *d_keep,
+                      void *d_workspace, const int32_t *d_indptr_sel, int32_t *d_indices_sel, int32_t *d_take,
+                      emg_stream_t stream);
+/* d_A_sel[q] = d_A[take[q]] (complex128), q < nnz_sel. */
+int emg_select_values(const emg_select *sel, const int32_t *d_take, const void *d_A, int64_t nnz, void *d_A_sel,
+                      emg_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
