@@ -24,7 +24,7 @@ EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
-    "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
+    "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
     "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values",
 )
 
@@ -50,6 +50,7 @@ class Plan(ctypes.Structure):
         ("off_order", ctypes.c_size_t),
         ("plan_bytes", ctypes.c_size_t),
         ("workspace_bytes", ctypes.c_size_t),
+        ("record_bytes", ctypes.c_int32),
     ]
 
 
@@ -109,6 +110,7 @@ def lib():
                                ctypes.c_int, _D, _D, _D, _D, _P, ctypes.c_size_t, _P, _P, _P]
     L.emg_form_sweep.argtypes = [_P, _P, _P, _I64, ctypes.POINTER(_D), ctypes.c_int, _P, _I64, _P]
     L.emg_form_batch.argtypes = [_P, _P, _P, ctypes.c_int, _P]
+    L.emg_plan_set_record_width.argtypes = [ctypes.POINTER(Plan), ctypes.c_int]
     L.emg_plan_order.argtypes = [ctypes.POINTER(Plan), _P, _P, _I64, _P, _P, _P, _P]
     L.emg_robin_init.argtypes = [_I64, ctypes.POINTER(Robin)]
     L.emg_robin_build.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P,
@@ -124,7 +126,7 @@ def lib():
                                        ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
     for name in ("emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
-                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_robin_init", "emg_robin_build",
+                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
                  "emg_select_values"):
         getattr(L, name).restype = ctypes.c_int

@@ -325,7 +325,7 @@ class GpuCSCMapping:
     sparsity pattern (indptr, indices: bit-identical to the reference's) and
     the column-gather plan, built once per mesh and assembled-tet set."""
 
-    def __init__(self, dmesh: DeviceMesh, chunk_order: str = "morton"):
+    def __init__(self, dmesh: DeviceMesh, chunk_order: str = "morton", record_bytes: int = 8):
         if chunk_order not in ("morton", "interleave"):
             raise ValueError(f"chunk_order must be 'morton' or 'interleave', got {chunk_order!r}")
         lib = L.lib()
@@ -337,6 +337,9 @@ class GpuCSCMapping:
                           None if m.tetids_host is None else hash(m.tetids_host.tobytes()))
         plan = L.Plan()
         L.check(lib.emg_plan_init(m.n_tets, m.n_assy, m.n_edges, m.n_tris, L.ctypes.byref(plan)))
+        if record_bytes == 4 and m.n_assy * 210 >= (1 << 31):
+            record_bytes = 8  # too many tets for the compact record
+        L.check(lib.emg_plan_set_record_width(L.ctypes.byref(plan), int(record_bytes)))
         self.plan = plan
         self.alloc = m.alloc
         self.d_plan = _empty(max(plan.plan_bytes, 1), torch.uint8, m.device, m.alloc)
@@ -459,5 +462,6 @@ def tet_mass_stiffness_matrices(field, er: np.ndarray, ur: np.ndarray, conductor
     dmat = DeviceMaterial(er, ur, dmesh.n_tets, dmesh.device)
     job = _Job(dmesh, dmat, _prec(precision))
     if cscmap is None:
-        cscmap = GpuCSCMapping(dmesh)
+        # compact 4-byte gather records are faster for complex128 element values
+        cscmap = GpuCSCMapping(dmesh, record_bytes=8 if job.precision == L.EMG_MIXED else 4)
     return ElemValues(job, "K"), ElemValues(job, "M"), cscmap

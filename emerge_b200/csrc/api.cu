@@ -89,6 +89,18 @@ int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tri
   p->n_ent = n_edges + n_tris;
   p->n_items = 10 * n_assy;
   p->N = 2 * (n_edges + n_tris);
+  p->record_bytes = 8;
+  plan_layout(p);
+  p->workspace_bytes = plan_workspace_bytes(p);
+  return EMG_OK;
+}
+
+int emg_plan_set_record_width(emg_plan *p, int bytes) {
+  if (!p) return fail(EMG_EINVAL, "null plan");
+  if (bytes != 4 && bytes != 8) return fail(EMG_EINVAL, "record width must be 4 or 8 bytes, got %d", bytes);
+  if (bytes == 4 && !pidx_compact_fits(p->n_assy))
+    return fail(EMG_ERANGE, "4-byte records address at most %lld assembled tets", (long long)((1LL << 31) / 210));
+  p->record_bytes = bytes;
   plan_layout(p);
   p->workspace_bytes = plan_workspace_bytes(p);
   return EMG_OK;

@@ -62,6 +62,35 @@ __host__ __device__ __forceinline__ int canon_dof(int ranks, int r) {
 // index of canonical pair (x, y), x <= y, in the packed upper triangle
 __host__ __device__ __forceinline__ int packed_index(int x, int y) { return x * (41 - x) / 2 + (y - x); }
 
+// Compact gather record (emg_plan.record_bytes = 4; one uint32 per
+// contribution instead of an int2 of both value indices): the packed index of
+// the contribution's first-column value, ia * 210 + p0, with bit 31 set when
+// the row DoF sorts first in p0's (min, max) pair. The owner entity's second
+// column DoF is its first plus 6 (edges) or 4 (faces), so p0 and that bit
+// determine the second value's slot p1 = kSecondSlot[bit][p0].
+struct SecondSlotTable {
+  uint8_t v[2][210];
+};
+constexpr SecondSlotTable make_second_slot_table() {
+  SecondSlotTable t{};
+  int lo_of[210] = {}, hi_of[210] = {};
+  for (int x = 0; x < 20; ++x)
+    for (int y = x; y < 20; ++y) {
+      lo_of[x * (41 - x) / 2 + (y - x)] = x;
+      hi_of[x * (41 - x) / 2 + (y - x)] = y;
+    }
+  for (int f = 0; f < 2; ++f)
+    for (int p = 0; p < 210; ++p) {
+      const int b0 = f ? hi_of[p] : lo_of[p], row = f ? lo_of[p] : hi_of[p];
+      const bool first = b0 < 6 || (b0 >= 12 && b0 < 16);
+      const int b1 = b0 < 6 ? b0 + 6 : b0 + 4;
+      const int x = row < b1 ? row : b1, y = row < b1 ? b1 : row;
+      t.v[f][p] = first ? (uint8_t)(x * (41 - x) / 2 + (y - x)) : (uint8_t)0;
+    }
+  return t;
+}
+__host__ __device__ __forceinline__ bool pidx_compact_fits(int64_t n_assy) { return n_assy * 210 < (1LL << 31); }
+
 // status word: [0] flags (EMG_ST_*), [1] smallest offending index
 __device__ __forceinline__ void flag(int64_t *st, int64_t bit, int64_t index) {
   if (st) {

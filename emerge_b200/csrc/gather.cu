@@ -125,24 +125,43 @@ __global__ void __launch_bounds__(PG_WARPS * 32)
 }
 
 // packed layout (the assembly path): per contribution the two value indices
-// come straight from the plan
-template <typename R>
+// come from the plan, as an int2 or as one compact uint32 (first index + a
+// bit, the second slot from kSecondSlot)
+__constant__ SecondSlotTable kSecondSlot = make_second_slot_table();
+
+template <typename R, bool COMPACT>
 __global__ void __launch_bounds__(PG_WARPS * 32)
-    k_gather_packed(const int32_t *ent_ptr, const int32_t *order, const int2 *pidx, const uint16_t *posoff,
-                    int64_t E, int64_t F, int64_t n_values, const int32_t *indptr, const void *v, double ar, double ai, double2 *A) {
+    k_gather_packed(const int32_t *ent_ptr, const int32_t *order, const void *pidx_v, const uint16_t *posoff,
+                    int64_t E, int64_t F, int64_t n_values, const int32_t *indptr, const void *v, double ar,
+                    double ai, double2 *A) {
+  __shared__ uint8_t slot2[2][210];
+  if constexpr (COMPACT) {
+    for (int i = threadIdx.x; i < 420; i += blockDim.x) slot2[i / 210][i % 210] = kSecondSlot.v[i / 210][i % 210];
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31;
   ChunkMeta m;
   if (!chunk_meta(ent_ptr, order, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
   const int total = 20 * (m.I1 - m.I0);
-  const int2 *plist = pidx + (int64_t)20 * m.I0;
   for (int p = lane; p < m.Lsum; p += 32) {
     const int o0 = posoff[m.hbase + p];
     const int o1 = min(p + 1 < m.Lsum ? (int)posoff[m.hbase + p + 1] : total, total);
     double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
     for (int k = o0; k < o1; ++k) {
-      const int2 q = __ldg(plist + k);
-      if ((uint32_t)q.x >= (uint64_t)n_values || (uint32_t)q.y >= (uint64_t)n_values) continue;
-      const C64 u0 = load_val<R>(v, q.x), u1 = load_val<R>(v, q.y);
+      int64_t qx, qy;
+      if constexpr (COMPACT) {
+        const uint32_t c = __ldg(static_cast<const uint32_t *>(pidx_v) + (int64_t)20 * m.I0 + k);
+        const uint32_t x = c & 0x7fffffffu;
+        const uint32_t p0 = x % 210u;
+        qx = x;
+        qy = (int64_t)(x - p0) + slot2[c >> 31][p0];
+      } else {
+        const int2 q = __ldg(static_cast<const int2 *>(pidx_v) + (int64_t)20 * m.I0 + k);
+        qx = (uint32_t)q.x;
+        qy = (uint32_t)q.y;
+      }
+      if (qx >= n_values || qy >= n_values) continue;
+      const C64 u0 = load_val<R>(v, qx), u1 = load_val<R>(v, qy);
       s0r += u0.re;
       s0i += u0.im;
       s1r += u1.re;
@@ -239,14 +258,18 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
   const bool f32 = values_fp32(precision);
   if (layout == EMG_LAYOUT_PACKED) {
     if (two) return fail(EMG_EINVAL, "the packed layout takes one value array");
-    const int2 *pidx = reinterpret_cast<const int2 *>(plan + p->off_pidx);
+    const void *pidx = plan + p->off_pidx;
     const int64_t nv = p->n_assy * 210;
-    if (f32)
-      k_gather_packed<float><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, order, pidx, posoff, p->n_edges, p->n_tris, nv,
-                                                         d_indptr, d_v1, ar, ai, A);
-    else
-      k_gather_packed<double><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, order, pidx, posoff, p->n_edges, p->n_tris, nv,
-                                                          d_indptr, d_v1, ar, ai, A);
+    const bool compact = p->record_bytes == 4;
+#define EMG_PK(R, C)                                                                                             \
+  k_gather_packed<R, C><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, order, pidx, posoff, p->n_edges, p->n_tris, nv, d_indptr, \
+                                                    d_v1, ar, ai, A)
+    if (f32) {
+      if (compact) EMG_PK(float, true); else EMG_PK(float, false);
+    } else {
+      if (compact) EMG_PK(double, true); else EMG_PK(double, false);
+    }
+#undef EMG_PK
     return launch_check("k_gather_packed");
   }
 #define EMG_COO(R, TWO)                                                                                           \

@@ -314,7 +314,8 @@ constexpr int CC_WARPS = 8;
 
 __global__ void __launch_bounds__(CC_WARPS * 32)
     k_chunk_contrib(const int32_t *ent_ptr, const Item *items, const uint32_t *ent_cnt, int64_t E, int64_t F,
-                    const int32_t *indptr, uint16_t *contrib, uint16_t *posoff, int2 *pidx, int64_t *st) {
+                    const int32_t *indptr, uint16_t *contrib, uint16_t *posoff, void *pidx_v, bool compact,
+                    int64_t *st) {
   __shared__ int32_t cnt_all[CC_WARPS][CHUNK_MAX_POS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t chunk = (int64_t)blockIdx.x * CC_WARPS + w;
@@ -383,8 +384,13 @@ __global__ void __launch_bounds__(CC_WARPS * 32)
           const int al = canon_dof(rec.ranks, r);
           const int b0 = canon_dof(rec.ranks, a0), b1 = canon_dof(rec.ranks, a1);
           const int64_t base = (int64_t)rec.ia * 210;
-          pidx[(int64_t)20 * I0 + at] = make_int2((int)(base + packed_index(min(al, b0), max(al, b0))),
-                                                  (int)(base + packed_index(min(al, b1), max(al, b1))));
+          if (compact)
+            static_cast<uint32_t *>(pidx_v)[(int64_t)20 * I0 + at] =
+                (uint32_t)(base + packed_index(min(al, b0), max(al, b0))) | (al <= b0 ? 0x80000000u : 0u);
+          else
+            static_cast<int2 *>(pidx_v)[(int64_t)20 * I0 + at] =
+                make_int2((int)(base + packed_index(min(al, b0), max(al, b0))),
+                          (int)(base + packed_index(min(al, b1), max(al, b1))));
         }
       }
       __syncwarp();
@@ -533,7 +539,7 @@ size_t plan_layout(emg_plan *p) {
   // per contribution the packed-layout indices of its two values (first- and
   // second-DoF column), in the same order as contrib
   p->off_pidx = o;
-  o = align_up(o + (size_t)p->n_items * 20 * 8, 256);
+  o = align_up(o + (size_t)p->n_items * 20 * (p->record_bytes == 4 ? 4 : 8), 256);
   // the gather's chunk processing order
   p->off_order = o;
   o = align_up(o + (size_t)n_chunks(p->n_edges, p->n_tris) * 4, 256);
@@ -639,9 +645,10 @@ int plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, c
   if (rc) return rc;
   uint16_t *contrib = reinterpret_cast<uint16_t *>(plan + p->off_contrib);
   uint16_t *posoff = reinterpret_cast<uint16_t *>(plan + p->off_posoff);
-  int2 *pidx = reinterpret_cast<int2 *>(plan + p->off_pidx);
+  void *pidx = plan + p->off_pidx;
+  const bool compact = p->record_bytes == 4;
   k_chunk_contrib<<<grid_for(n_chunks(p->n_edges, p->n_tris), CC_WARPS), CC_WARPS * 32, 0, s>>>(
-      ent_ptr, items, ent_cnt, p->n_edges, p->n_tris, d_indptr, contrib, posoff, pidx, d_status);
+      ent_ptr, items, ent_cnt, p->n_edges, p->n_tris, d_indptr, contrib, posoff, pidx, compact, d_status);
   return launch_check("k_chunk_contrib");
 }
 

@@ -118,6 +118,7 @@ typedef struct {
   size_t off_order;       /* int32 per entity chunk: the gather's processing order */
   size_t plan_bytes;      /* blob size */
   size_t workspace_bytes; /* scratch needed by emg_plan_build and emg_plan_order */
+  int32_t record_bytes;   /* 8 (default) or 4: bytes per contribution record of the packed gather */
 } emg_plan;
 
 int emg_version(void);
@@ -134,6 +135,15 @@ int emg_status_read(const int64_t *d_status, int64_t *h_flags, int64_t *h_first_
 /* Host-only: sizes and blob offsets for a mesh. Replaces the allocation part
  * of CSCMapping.from_rowcol (csc_cast.py:51-53). */
 int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tris, emg_plan *plan);
+
+/* Host-only, between emg_plan_init and emg_plan_build: the width of the
+ * packed gather's per-contribution record. 8 bytes (default) store both value
+ * indices; 4 bytes store the first and a bit, the second is derived on chip
+ * (at most 10,226,078 assembled tets). 4 bytes halve that stream and are
+ * faster for complex128 element values (plain FP64 / exact), 8 bytes are
+ * faster for complex64 (mixed). Values are identical either way. Updates
+ * plan_bytes. No counterpart in the reference. */
+int emg_plan_set_record_width(emg_plan *plan, int bytes);
 
 /* Builds the entity->tet incidence lists, column lengths and indptr[N+1]
  * (int32) on the device, then synchronises `stream` and stores nnz/max_col in

@@ -136,17 +136,19 @@ def test_mapping_rejects_other_mesh():
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_chunk_order_changes_no_value(mid_case, precision):
     """The Morton processing order of the gather's entity chunks and the
-    default interleave give bitwise identical A (same sums, other warps)."""
+    default interleave, with 8- or 4-byte contribution records, give bitwise
+    identical A (same sums, other warps)."""
     f, er, ur = mid_case[0], mid_case[1], mid_case[2]
     from emerge_b200.assembly import DeviceMaterial, DeviceMesh, _Job, _prec
 
     dm = DeviceMesh(f, np.zeros(0, np.int64))
     job = _Job(dm, DeviceMaterial(er, ur, dm.n_tets, dm.device), _prec(precision))
     outs = []
-    for order in ("interleave", "morton"):
-        cm = GpuCSCMapping(dm, chunk_order=order)
+    for order, width in (("interleave", 8), ("morton", 8), ("morton", 4), ("interleave", 4)):
+        cm = GpuCSCMapping(dm, chunk_order=order, record_bytes=width)
         outs.append(cm.assemble_device(job, 1.0 + 0j, -2345.5 + 1.25j)[: cm.nnz].cpu().numpy())
         dm.check_status()
-    assert np.array_equal(outs[0], outs[1])
+    for o in outs[1:]:
+        assert np.array_equal(outs[0], o)
     with pytest.raises(ValueError):
         GpuCSCMapping(dm, chunk_order="hilbert")

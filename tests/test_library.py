@@ -32,5 +32,10 @@ def test_host_only_entry_points():
     assert p.N == 88296 and p.n_items == 129600 and p.plan_bytes > 0 and p.workspace_bytes > 0
     assert lib.emg_plan_init(-1, 0, 0, 0, ctypes.byref(p)) == L.EMG_EINVAL
     assert b"negative" in lib.emg_last_error()
+    assert p.record_bytes == 8
+    wide = p.plan_bytes
+    assert lib.emg_plan_set_record_width(ctypes.byref(p), 4) == 0 and p.record_bytes == 4
+    assert p.plan_bytes < wide
+    assert lib.emg_plan_set_record_width(ctypes.byref(p), 3) == L.EMG_EINVAL
     assert lib.emg_assemble_workspace_size(10, L.EMG_FP64) == 10 * 210 * 16
     assert lib.emg_assemble_workspace_size(10, L.EMG_MIXED) == 10 * 210 * 8
