@@ -25,7 +25,8 @@ EXPORTS = (
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
     "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
-    "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values",
+    "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values", "emg_ned2_interp",
+    "emg_port_overlap",
 )
 
 
@@ -120,6 +121,9 @@ def lib():
     L.emg_select_build.argtypes = [ctypes.POINTER(Select), _P, _P, _P, _P, _P, _P, _P]
     L.emg_select_finish.argtypes = [ctypes.POINTER(Select), _P, _P, _P, _P, _P, _P, _P, _P]
     L.emg_select_values.argtypes = [ctypes.POINTER(Select), _P, _P, _I64, _P, _P]
+    L.emg_ned2_interp.argtypes = [_P, _I64, _P, _I64, _P, _P, _I64, _I64, _P, _P, _I64, _P, _P, _P]
+    L.emg_port_overlap.argtypes = [_P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, ctypes.c_int, _P,
+                                   _D, _P, _P, _P, _P]
     L.emg_robin_force.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P,
                                   _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
@@ -128,7 +132,7 @@ def lib():
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
                  "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
-                 "emg_select_values"):
+                 "emg_select_values", "emg_ned2_interp", "emg_port_overlap"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

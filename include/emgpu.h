@@ -330,6 +330,28 @@ int emg_select_finish(const emg_select *sel, const int32_t *d_indptr, const int3
 int emg_select_values(const emg_select *sel, const int32_t *d_take, const void *d_A, int64_t nnz, void *d_A_sel,
                       emg_stream_t stream);
 
+/* Post-processing. The solution d_x (complex128 [N]) at points d_points
+ * (f64 [3][n_points]) inside the tets d_tet_of (int32 [n_points]; -1 or an
+ * invalid tet gives NaN, as the reference does for points outside): d_E
+ * complex128 [3][n_points]. Replaces ned2_tet_interp
+ * (compiled/base/interp.py:286-387) for points whose tet is known. */
+int emg_ned2_interp(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
+                    const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri, int64_t n_edges, int64_t n_tris,
+                    const void *d_x, const double *d_points, int64_t n_points, const int32_t *d_tet_of, void *d_E,
+                    emg_stream_t stream);
+
+/* Port overlap of the S-parameters: per port triangle d_btris[i] (lying on a
+ * face of tet d_btets[i]) area * sum_k w_k (E - q U) . conj(U) at the points
+ * of the triangle rule h_rule (host f64 [4][nq]: weights, L1, L2, L3; nq <=
+ * 16), U complex128 [3][nq][n_btris]; d_per_tri complex128 [n_btris] and
+ * *d_total their sum (fixed order). The integral of sparam_field_power
+ * (physics/microwave/sparam.py:62-97, mth/integrals.py:64-103) times 2 Z0. */
+int emg_port_overlap(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
+                     const int32_t *d_tet_to_edge, const int32_t *d_tet_to_tri, const int32_t *d_tris, int64_t n_edges,
+                     int64_t n_tris, const void *d_x, const int32_t *d_btris, const int32_t *d_btets, int64_t n_btris,
+                     const double *h_rule, int nq, const void *d_U, double q, void *d_per_tri, void *d_total,
+                     int64_t *d_status, emg_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,8 @@ surface on numpy arrays:
 * ``tri_stiff``, ``robin_entries``, ``tri_rowcol``, ``generate_csc``
                        -> robinbc.py:316-402 (``ned2_tri_stiff``,
                           ``compute_bc_entries``), femdata.py:52-56,75-92,104-118
+* ``ned2_interp``, ``port_overlap`` -> compiled/base/interp.py:286-387,
+                          mth/integrals.py:13-24,64-103, sparam.py:62-97
 * ``tri_force``, ``force_entries``, ``tri_points`` -> robinbc.py:104-135,220-313
                           (``generate_points_3d``, ``ned2_tri_force``,
                           ``compute_force_entries``)
@@ -71,6 +73,11 @@ def lib():
         L.oracle_robin_entries.argtypes = [_p, _i64, _p, _i64, _p, _i64, ctypes.c_double, ctypes.c_double, _p]
         L.oracle_tri_force.restype = None
         L.oracle_tri_force.argtypes = [_p, _p, _p]
+        L.oracle_ned2_interp.restype = None
+        L.oracle_ned2_interp.argtypes = [_p, _i64, _p, _i64, _p, _i64, _p, _i64, _p, _p, _p, _p, _i64, _p, _p]
+        L.oracle_port_overlap.restype = None
+        L.oracle_port_overlap.argtypes = [_p, _i64, _p, _i64, _p, _i64, _p, _i64, _p, _p, _p, _p, _p, _i64, _p,
+                                          ctypes.c_int, _p, ctypes.c_double, _p, _p]
         L.oracle_force_entries.restype = ctypes.c_int
         L.oracle_force_entries.argtypes = [_p, _i64, _p, _i64, _p, _p, _i64, _p, _i64, _p]
         _lib = L
@@ -302,3 +309,44 @@ def force_entries(field, tri_ids, U: np.ndarray, b: np.ndarray | None = None) ->
     if rc != 0:
         raise IndexError("tri id or index out of range")
     return b
+
+
+# ---------------------------------------------------------------- post-processing
+def _mesh_args(field):
+    m = field.mesh
+    c = np.ascontiguousarray
+    return (c(m.nodes, dtype=np.float64), m.n_nodes, c(m.tets, dtype=np.int64), m.n_tets, c(m.edges, dtype=np.int64),
+            m.n_edges, c(m.tris, dtype=np.int64), m.n_tris, c(m.tet_to_edge, dtype=np.int64),
+            c(m.tet_to_tri, dtype=np.int64))
+
+
+def ned2_interp(field, x, points, tet_of) -> np.ndarray:
+    """``ned2_tet_interp`` (interp.py:286-387): the solution x (c16[N]) at
+    points f8[3, n] inside tets tet_of (i8[n], -1 = outside -> NaN) ->
+    c16[3, n]."""
+    a = _mesh_args(field)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    t = np.ascontiguousarray(tet_of, dtype=np.int64)
+    out = np.empty((3, pts.shape[1]), np.complex128)
+    lib().oracle_ned2_interp(*[(_ptr(v) if isinstance(v, np.ndarray) else v) for v in a], _ptr(x), _ptr(pts),
+                             pts.shape[1], _ptr(t), _ptr(out))
+    return out
+
+
+def port_overlap(field, x, tri_ids, tri_tets, rule, U, q: float):
+    """sum over tris of area * sum_k w_k (E - q U) . conj(U) at the rule's
+    points (surface_integral with unit constants of sparam_field_power's
+    integrand times 2 Z0); rule f8[4, nq] (weights, L1, L2, L3), U
+    c16[3, nq, nb]. Returns (total, per-tri c16[nb])."""
+    a = _mesh_args(field)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    ids = np.ascontiguousarray(tri_ids, dtype=np.int64)
+    tt = np.ascontiguousarray(tri_tets, dtype=np.int64)
+    rule = np.ascontiguousarray(rule, dtype=np.float64)
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    per = np.empty(ids.size, np.complex128)
+    tot = np.zeros(1, np.complex128)
+    lib().oracle_port_overlap(*[(_ptr(v) if isinstance(v, np.ndarray) else v) for v in a], _ptr(x), _ptr(ids),
+                              _ptr(tt), ids.size, _ptr(rule), rule.shape[1], _ptr(U), float(q), _ptr(per), _ptr(tot))
+    return complex(tot[0]), per

@@ -20,6 +20,8 @@ modules directly:
 * ``emerge._emerge.mth.optimized`` (``local_mapping`` :262-296, ``matinv`` :315-357)
 * ``emerge._emerge.physics.microwave.assembly.robinbc`` (``ned2_tri_stiff``
   :316-378, ``compute_bc_entries`` :381-402)
+* ``emerge._emerge.compiled.base.interp`` (``ned2_tet_interp`` :286-387) and
+  ``emerge._emerge.mth.integrals`` (``surface_integral`` :64-103)
 """
 from __future__ import annotations
 
@@ -66,4 +68,9 @@ def load_reference(ref_root: str = DEFAULT_REF_ROOT):
     ns.ccbf = importlib.import_module("emerge._emerge.compiled.ccbf")
     # Robin boundary term (robinbc.py); imports cleanly with the stubs above
     ns.robinbc = importlib.import_module("emerge._emerge.physics.microwave.assembly.robinbc")
+    # post-processing: field interpolation and surface integrals
+    if "emerge._emerge.compiled.base" not in sys.modules:
+        _pkg("emerge._emerge.compiled.base", os.path.join(em, "compiled", "base"))
+    ns.interp = importlib.import_module("emerge._emerge.compiled.base.interp")
+    ns.integrals = importlib.import_module("emerge._emerge.mth.integrals")
     return ns

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     src = open(os.path.join(ROOT, "include", "emgpu.h")).read()
-    return sorted(set(re.findall(r"\b(emg_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(emg_[a-z0-9_]+)\s*\(", src)))
 
 
 def test_header_matches_binding_list():
