@@ -10,6 +10,8 @@ surface on numpy arrays:
 * ``tri_stiff``, ``robin_entries``, ``tri_rowcol``, ``generate_csc``
                        -> robinbc.py:316-402 (``ned2_tri_stiff``,
                           ``compute_bc_entries``), femdata.py:52-56,75-92,104-118
+* ``leg2_values``, ``leg2_rowcol`` -> physics/heatconduction/assembly/grad.py:
+                          199-400 (Lagrange-2 heat stiffness / mass, COO)
 * ``ned2_interp``, ``port_overlap`` -> compiled/base/interp.py:286-387,
                           mth/integrals.py:13-24,64-103, sparam.py:62-97
 * ``tri_force``, ``force_entries``, ``tri_points`` -> robinbc.py:104-135,220-313
@@ -73,6 +75,8 @@ def lib():
         L.oracle_robin_entries.argtypes = [_p, _i64, _p, _i64, _p, _i64, ctypes.c_double, ctypes.c_double, _p]
         L.oracle_tri_force.restype = None
         L.oracle_tri_force.argtypes = [_p, _p, _p]
+        L.oracle_leg2_builder.restype = ctypes.c_int
+        L.oracle_leg2_builder.argtypes = [_p, _i64, _p, _i64, _p, ctypes.c_int, _p]
         L.oracle_ned2_interp.restype = None
         L.oracle_ned2_interp.argtypes = [_p, _i64, _p, _i64, _p, _i64, _p, _i64, _p, _p, _p, _p, _i64, _p, _p]
         L.oracle_port_overlap.restype = None
@@ -350,3 +354,27 @@ def port_overlap(field, x, tri_ids, tri_tets, rule, U, q: float):
     lib().oracle_port_overlap(*[(_ptr(v) if isinstance(v, np.ndarray) else v) for v in a], _ptr(x), _ptr(ids),
                               _ptr(tt), ids.size, _ptr(rule), rule.shape[1], _ptr(U), float(q), _ptr(per), _ptr(tot))
     return complex(tot[0]), per
+
+
+# ---------------------------------------------------------------- heat conduction (Lagrange-2)
+def leg2_values(mesh, coef, kind: str) -> np.ndarray:
+    """``_stiff_matrix_builder`` (kind 'stiff', coef = conductivity f8[3, 3, nT])
+    or ``_mass_matrix_builder`` (kind 'mass', coef = rho_cp f8[nT]),
+    grad.py:333-400: the COO values f8[100 nT]."""
+    nodes = np.ascontiguousarray(mesh.nodes, dtype=np.float64)
+    tets = np.ascontiguousarray(mesh.tets, dtype=np.int64)
+    c = np.ascontiguousarray(coef, dtype=np.float64)
+    out = np.empty(100 * tets.shape[1])
+    lib().oracle_leg2_builder(_ptr(nodes), nodes.shape[1], _ptr(tets), tets.shape[1], _ptr(c),
+                              0 if kind == "stiff" else 1, _ptr(out))
+    return out
+
+
+def leg2_rowcol(tet_to_field: np.ndarray):
+    """COO rows/cols of grad.py:350-354: per tet 100 slots, rows[p + 10 ii +
+    jj] = t2f[ii], cols[p + 10 ii + jj] = t2f[jj]."""
+    t = np.asarray(tet_to_field).T  # (nT, 10)
+    nT = t.shape[0]
+    rows = np.repeat(t[:, :, None], 10, axis=2).reshape(nT * 100)
+    cols = np.repeat(t[:, None, :], 10, axis=1).reshape(nT * 100)
+    return rows, cols

@@ -20,6 +20,8 @@ modules directly:
 * ``emerge._emerge.mth.optimized`` (``local_mapping`` :262-296, ``matinv`` :315-357)
 * ``emerge._emerge.physics.microwave.assembly.robinbc`` (``ned2_tri_stiff``
   :316-378, ``compute_bc_entries`` :381-402)
+* ``emerge._emerge.physics.heatconduction.assembly.grad`` (``leg2_tet_stiff``
+  :199-260, ``leg2_tet_mass`` :263-330, the COO builders :333-400)
 * ``emerge._emerge.compiled.base.interp`` (``ned2_tet_interp`` :286-387) and
   ``emerge._emerge.mth.integrals`` (``surface_integral`` :64-103)
 """
@@ -72,5 +74,14 @@ def load_reference(ref_root: str = DEFAULT_REF_ROOT):
     if "emerge._emerge.compiled.base" not in sys.modules:
         _pkg("emerge._emerge.compiled.base", os.path.join(em, "compiled", "base"))
     ns.interp = importlib.import_module("emerge._emerge.compiled.base.interp")
+    # heat conduction (grad.py imports Legrange2 as a type hint only)
+    if "emerge._emerge.physics.heatconduction.assembly.grad" not in sys.modules:
+        _pkg("emerge._emerge.physics.heatconduction", os.path.join(em, "physics", "heatconduction"))
+        _pkg("emerge._emerge.physics.heatconduction.assembly",
+             os.path.join(em, "physics", "heatconduction", "assembly"))
+        leg2 = types.ModuleType("emerge._emerge.elements.leg2")
+        leg2.Legrange2 = object
+        sys.modules["emerge._emerge.elements.leg2"] = leg2
+    ns.heat = importlib.import_module("emerge._emerge.physics.heatconduction.assembly.grad")
     ns.integrals = importlib.import_module("emerge._emerge.mth.integrals")
     return ns
