@@ -26,7 +26,8 @@ EXPORTS = (
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
     "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
     "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values", "emg_ned2_interp",
-    "emg_port_overlap",
+    "emg_port_overlap", "emg_coo_init", "emg_coo_rowcol", "emg_coo_build", "emg_coo_finish", "emg_coo_gather",
+    "emg_leg2_element",
 )
 
 
@@ -64,6 +65,11 @@ class Robin(ctypes.Structure):
 class Select(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int64), ("M", ctypes.c_int64), ("nnz_sel", ctypes.c_int64),
                 ("workspace_bytes", ctypes.c_size_t)]
+
+
+class CooMap(ctypes.Structure):
+    _fields_ = [("S", ctypes.c_int64), ("N", ctypes.c_int64), ("nnz", ctypes.c_int64), ("perm_bytes", ctypes.c_size_t),
+                ("run_bytes", ctypes.c_size_t), ("workspace_bytes", ctypes.c_size_t)]
 
 
 class FormItem(ctypes.Structure):
@@ -124,6 +130,12 @@ def lib():
     L.emg_ned2_interp.argtypes = [_P, _I64, _P, _I64, _P, _P, _I64, _I64, _P, _P, _I64, _P, _P, _P]
     L.emg_port_overlap.argtypes = [_P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, ctypes.c_int, _P,
                                    _D, _P, _P, _P, _P]
+    L.emg_coo_init.argtypes = [_I64, _I64, ctypes.POINTER(CooMap)]
+    L.emg_coo_rowcol.argtypes = [_P, ctypes.c_int, _I64, _P, _P, _P]
+    L.emg_coo_build.argtypes = [ctypes.POINTER(CooMap), _P, _P, _P, _P, _P, _P, _P]
+    L.emg_coo_finish.argtypes = [ctypes.POINTER(CooMap), _P, _P, _P, _P, _P, _P, _P]
+    L.emg_coo_gather.argtypes = [ctypes.POINTER(CooMap), _P, _P, ctypes.c_int, _P, _P, _P]
+    L.emg_leg2_element.argtypes = [_P, _I64, _P, _I64, _P, ctypes.c_int, _P, _P, _P]
     L.emg_robin_force.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P,
                                   _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
@@ -132,7 +144,8 @@ def lib():
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
                  "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
-                 "emg_select_values", "emg_ned2_interp", "emg_port_overlap"):
+                 "emg_select_values", "emg_ned2_interp", "emg_port_overlap", "emg_coo_init", "emg_coo_rowcol",
+                 "emg_coo_build", "emg_coo_finish", "emg_coo_gather", "emg_leg2_element"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -352,6 +352,39 @@ int emg_port_overlap(const double *d_nodes, int64_t n_nodes, const int32_t *d_te
                      const double *h_rule, int nq, const void *d_U, double q, void *d_per_tri, void *d_total,
                      int64_t *d_status, emg_stream_t stream);
 
+/* General COO -> CSC mapping: CSCMapping.from_rowcol / to_csc
+ * (mth/csc_cast.py:51-177) for any slot list, as the heat-conduction assembly
+ * uses it (physics/heatconduction/assembly/grad.py:403-460). Slots are
+ * counted and scattered per column, each column's slots sorted by (row, slot)
+ * (a fixed order), its distinct rows are its entries; an entry's value is the
+ * sum of its slots in that order. Sizes from emg_coo_init: d_perm perm_bytes,
+ * d_run run_bytes, workspace workspace_bytes (keep it from build to finish),
+ * d_indptr N + 1, d_indices nnz (set by emg_coo_build, which synchronises). */
+typedef struct {
+  int64_t S, N, nnz;
+  size_t perm_bytes, run_bytes, workspace_bytes;
+} emg_coo_map;
+
+int emg_coo_init(int64_t n_slots, int64_t N, emg_coo_map *map);
+/* rows/cols of an element with D DoFs per tet: slot D^2 t + D ii + jj has row
+ * t2f[ii] and column t2f[jj] (femdata.py:58-73); t2f int32 [D][n_tets]. */
+int emg_coo_rowcol(const int32_t *d_tet_to_field, int dofs_per_tet, int64_t n_tets, int32_t *d_rows, int32_t *d_cols,
+                   emg_stream_t stream);
+int emg_coo_build(emg_coo_map *map, const int32_t *d_rows, const int32_t *d_cols, int32_t *d_perm, void *d_workspace,
+                  int32_t *d_indptr, int64_t *d_status, emg_stream_t stream);
+int emg_coo_finish(const emg_coo_map *map, const int32_t *d_rows, const int32_t *d_perm, void *d_workspace,
+                   const int32_t *d_indptr, int32_t *d_indices, int32_t *d_run, emg_stream_t stream);
+/* CSC values (f64, or complex128 when is_complex) from slot values. */
+int emg_coo_gather(const emg_coo_map *map, const int32_t *d_perm, const int32_t *d_run, int is_complex,
+                   const void *d_values, void *d_out, emg_stream_t stream);
+
+/* Heat conduction, Lagrange-2 (10 DoFs per tet): per tet the 10x10 block in
+ * the reference's COO slots (row-major), kind 0 = stiffness with the
+ * conductivity d_coef f64 [3][3][n_tets] (leg2_tet_stiff, grad.py:199-260),
+ * kind 1 = mass with d_coef = rho_cp f64 [n_tets] (leg2_tet_mass :263-330). */
+int emg_leg2_element(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
+                     const double *d_coef, int kind, double *d_values, int64_t *d_status, emg_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
