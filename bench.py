@@ -51,6 +51,9 @@ def parse():
                     help="anisotropic PML shell + 2%% slivers (1,008,000 tets): speed and mixed-vs-FP64 errors")
     ap.add_argument("--shard", action="store_true",
                     help="strong scaling: one assembly column-sharded over the ranks instead of one replica per rank")
+    ap.add_argument("--heat", action="store_true",
+                    help="Lagrange-2 heat-conduction assembly (stiffness + capacity, COO -> CSC) on a 2.01M-tet box")
+    ap.add_argument("--heat-grid", default="100,50,67")
     ap.add_argument("--serving", action="store_true",
                     help="serving stream instead: Poisson arrivals of assembly jobs (5k-500k tets, 1-64 frequencies)")
     ap.add_argument("--serving-jobs", type=int, default=50)
@@ -521,6 +524,180 @@ def run_pml(args, rank, world, local_rank):
             "mixed_vs_fp64_errors": errors, "clocks": sampler.summary(), "gpu_launches": 4 * args.steps}
 
 
+def run_heat(args, rank, world, local_rank):
+    """--heat: the transient heat assembly of assembler.py:123-130 on a
+    Lagrange-2 box -- stiffness and capacity element values, each gathered
+    into CSC values -- with the field's mesh and COO -> CSC mapping resident.
+    Both element forms are timed ('fp64' = the reference's quadrature loop,
+    'exact' = the moment form); the line's value is the exact form."""
+    import torch
+
+    from emerge_b200 import _lib as L
+    from emerge_b200 import workloads as W
+    from emerge_b200.heat import _heat_mesh, tet_mass_matrix, tet_stiffness_matrix
+    from emerge_b200.ranks import max_over_ranks
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = W.heat_box(n=tuple(int(x) for x in args.heat_grid.split(",")))
+    f = wl.field
+    t0 = time.perf_counter()
+    hm = _heat_mesh(f, dev)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    cm = hm.cmap
+    nT, nN, nnz = hm.n_tets, hm.n_nodes, cm.nnz
+    d_cond = torch.from_numpy(wl.cond).to(dev)
+    d_rho = torch.from_numpy(wl.rho_cp).to(dev)
+    vK = torch.empty(100 * nT, dtype=torch.float64, device=dev)
+    vM = torch.empty(100 * nT, dtype=torch.float64, device=dev)
+    oK = torch.empty(nnz, dtype=torch.float64, device=dev)
+    oM = torch.empty(nnz, dtype=torch.float64, device=dev)
+    status = torch.zeros(2, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = L.ctypes.c_void_p(stream.cuda_stream)
+    lib = L.lib()
+
+    def elem(coef, kind, prec, out):
+        L.check(lib.emg_leg2_element(L.ptr(hm.nodes), nN, L.ptr(hm.tets), nT, L.ptr(coef), kind, prec,
+                                     L.EMG_LAYOUT_COO_T, L.ptr(out), L.ptr(status), sh))
+
+    def gath(v, out):
+        L.check(lib.emg_coo_gather(L.ctypes.byref(cm.desc), L.ptr(cm.d_perm), L.ptr(cm.d_run), 0, 10, L.ptr(v),
+                                   L.ptr(out), sh))
+
+    def ktime(fn, reps=5):
+        fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    res = {}
+    sampler = ClockSampler(local_rank)
+    for pname, prec in (("fp64", L.EMG_FP64), ("exact", L.EMG_EXACT)):
+        def step():
+            elem(d_cond, 0, prec, vK)
+            elem(d_rho, 1, prec, vM)
+            gath(vK, oK)
+            gath(vM, oM)
+
+        if pname == "exact":
+            sampler.__enter__()
+        ms = time_steps(step, args.steps, args.warmup, stream)
+        if pname == "exact":
+            sampler.__exit__()
+        ms = max_over_ranks([ms], dev)[0]
+        res[pname] = {"ms": ms, "k_stiff_ms": ktime(lambda: elem(d_cond, 0, prec, vK)),
+                      "k_mass_ms": ktime(lambda: elem(d_rho, 1, prec, vM)), "k_gather_ms": ktime(lambda: gath(vK, oK))}
+    fl, ix = L.ctypes.c_int64(), L.ctypes.c_int64()
+    L.check(lib.emg_status_read(L.ptr(status), L.ctypes.byref(fl), L.ctypes.byref(ix), sh))
+    if fl.value:
+        raise RuntimeError(f"heat workload flagged tet {ix.value}")
+    # the two forms agree on this workload
+    elem(d_cond, 0, L.EMG_FP64, vK)
+    elem(d_cond, 0, L.EMG_EXACT, vM)
+    form_diff = float((vK - vM).abs().max() / vK.abs().max())
+    # e2e: the public API, host arrays in, host csc_matrix out, field resident
+    e2e = None
+    if args.e2e_steps > 0:
+        def api():
+            K, c = tet_stiffness_matrix(f, wl.cond, precision="exact", device=dev)
+            A = c.to_csc(K)
+            M, c = tet_mass_matrix(f, wl.rho_cp, precision="exact", device=dev)
+            B = c.to_csc(M)
+            return A, B
+
+        api()
+        times = []
+        for _ in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            A, B = api()
+            times.append(time.perf_counter() - t1)
+            del A, B
+        t = max_over_ranks([float(np.median(times))], dev)[0]
+        e2e = {"value": world * nT / t, "unit": "tets/s", "h2d_bytes_per_step": int(wl.cond.nbytes + wl.rho_cp.nbytes),
+               "d2h_bytes_per_step": int(2 * nnz * 8), "s_per_step": t,
+               "path": "tet_stiffness_matrix + to_csc, tet_mass_matrix + to_csc -> scipy csc_matrix (mesh and "
+                       "mapping resident)"}
+    if rank != 0:
+        return None, None
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    src = "measured" if peaks.get("hbm_gbs") else "fallback"
+
+    def roof(r):
+        kb = {"k_leg2_stiff": W.heat_element_alg_bytes(nN, nT, "stiff"),
+              "k_leg2_mass": W.heat_element_alg_bytes(nN, nT, "mass"), "k_coo_gather": W.heat_gather_alg_bytes(nT, nnz)}
+        kms = {"k_leg2_stiff": r["k_stiff_ms"], "k_leg2_mass": r["k_mass_ms"], "k_coo_gather": r["k_gather_ms"]}
+        kern = {k: {"alg_bytes": kb[k], "ms": kms[k], "achieved": kb[k] / (kms[k] * 1e-3) / 1e9,
+                    "frac": kb[k] / (kms[k] * 1e-3) / 1e9 / hbm} for k in kb}
+        dom = max(kms, key=kms.get)
+        d = kern[dom]
+        return {"bound": "hbm", "kernel": dom, "achieved": d["achieved"], "peak": hbm, "unit": "GB/s",
+                "frac": d["frac"], "traffic": None, "peak_source": src, "alg_bytes_per_launch": d["alg_bytes"],
+                "kernels": kern}
+
+    ex, fp = res["exact"], res["fp64"]
+    line = {"metric": "tets/s assembled, Lagrange-2 heat conduction (stiffness + capacity, COO -> CSC)",
+            "value": world * nT / (ex["ms"] * 1e-3), "unit": "tets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ex["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl.name, "tets": nT, "hex_grid": list(wl.hex_grid), "N": int(f.n_field),
+                       "nnz": nnz, "form": "exact", "setup_s": setup_s,
+                       "l2": "inputs larger than L2 (1.6 GB of element values per matrix)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 gpu"},
+            "plain_fp64": {"value": world * nT / (fp["ms"] * 1e-3), "ms_per_step": fp["ms"],
+                           "k_stiff_ms": fp["k_stiff_ms"], "k_mass_ms": fp["k_mass_ms"],
+                           "note": "the reference's quadrature loop: FP64-arithmetic bound"},
+            "kernels_ms": {k: v for k, v in ex.items() if k != "ms"}, "exact_vs_fp64_max_rel": form_diff,
+            "roofline": roof(ex), "clocks": sampler.summary(), "e2e": e2e, "gpu_launches": 4 * args.steps}
+    return line, wl
+
+
+class HeatCpuBaseline:
+    """The reference's heat assembly restated in C (oracle/, OpenMP over all
+    host cores) on a bounded sample of the workload's tets: both element
+    builders and the f8 scatter of each into CSC, the sample's pattern
+    cached."""
+
+    def __init__(self, wl, sample_tets: int):
+        from oracle import oracle as O
+
+        self.O = O
+        f = wl.field
+        nT = f.mesh.n_tets
+        self.n = n = min(sample_tets, nT)
+        lo = (nT - n) // 2
+        sl = slice(lo, lo + n)
+        self.mesh = type("SampleMesh", (), {"nodes": f.mesh.nodes, "tets": np.ascontiguousarray(f.mesh.tets[:, sl])})()
+        self.cond = np.ascontiguousarray(wl.cond[:, :, sl])
+        self.rho = np.ascontiguousarray(wl.rho_cp[sl])
+        self.cores = os.cpu_count() or 1
+        rows, cols = O.leg2_rowcol(f.tet_to_field[:, sl])
+        self.pat = O.CSCPattern.from_rowcol(rows, cols, f.n_field, self.cores)
+        self.desc = (f"{n} contiguous tets of the {wl.name} workload ({nT} tets): stiffness and capacity element "
+                     f"builds + f8 scatter of each, pattern cached, {self.cores} threads")
+
+    def step(self):
+        t0 = time.perf_counter()
+        K = self.O.leg2_values(self.mesh, self.cond, "stiff")
+        M = self.O.leg2_values(self.mesh, self.rho, "mass")
+        self.pat.values_f8(K, self.cores)
+        self.pat.values_f8(M, self.cores)
+        return time.perf_counter() - t0
+
+    def measure(self, reps: int = 3):
+        self.step()
+        t = float(np.median([self.step() for _ in range(reps)]))
+        return {"value": self.n / t, "unit": "tets/s", "cores": self.cores, "kind": "port", "sample": self.desc}
+
+
 def run_shard(args, rank, world, local_rank):
     """--shard: the workload's columns split over the ranks (each rank
     assembles the tets touching its edges/faces, no exchange step); one step
@@ -625,10 +802,13 @@ def main():
         line, wl = run_sweep(args, rank, world, local_rank), None
     elif args.pml:
         line, wl = run_pml(args, rank, world, local_rank), None
+    elif args.heat:
+        line, wl = run_heat(args, rank, world, local_rank)
     else:
         line, wl = run_ours(args, rank, world, local_rank)
     if rank == 0 and not args.no_cpu_baseline and wl is not None:
-        line["cpu_baseline"] = CpuBaseline(wl, args.cpu_sample_tets).measure()
+        base = HeatCpuBaseline if args.heat else CpuBaseline
+        line["cpu_baseline"] = base(wl, args.cpu_sample_tets).measure()
     if world > 1:
         import torch.distributed as dist
 

@@ -17,7 +17,7 @@ EMG_ST_INDEX, EMG_ST_DEGENERATE, EMG_ST_CAPACITY = 1, 2, 4
 EMG_MAT_ISO, EMG_MAT_DIAG, EMG_MAT_FULL = 0, 1, 2
 EMG_FP64, EMG_MIXED, EMG_EXACT = 0, 1, 2
 EMG_OUT_LINCOMB, EMG_OUT_K, EMG_OUT_M = 0, 1, 2
-EMG_LAYOUT_COO, EMG_LAYOUT_PACKED = 0, 1
+EMG_LAYOUT_COO, EMG_LAYOUT_PACKED, EMG_LAYOUT_COO_T = 0, 1, 2
 
 # every symbol include/emgpu.h declares
 EXPORTS = (
@@ -134,8 +134,8 @@ def lib():
     L.emg_coo_rowcol.argtypes = [_P, ctypes.c_int, _I64, _P, _P, _P]
     L.emg_coo_build.argtypes = [ctypes.POINTER(CooMap), _P, _P, _P, _P, _P, _P, _P]
     L.emg_coo_finish.argtypes = [ctypes.POINTER(CooMap), _P, _P, _P, _P, _P, _P, _P]
-    L.emg_coo_gather.argtypes = [ctypes.POINTER(CooMap), _P, _P, ctypes.c_int, _P, _P, _P]
-    L.emg_leg2_element.argtypes = [_P, _I64, _P, _I64, _P, ctypes.c_int, _P, _P, _P]
+    L.emg_coo_gather.argtypes = [ctypes.POINTER(CooMap), _P, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P]
+    L.emg_leg2_element.argtypes = [_P, _I64, _P, _I64, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P]
     L.emg_robin_force.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P,
                                   _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),

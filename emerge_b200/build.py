@@ -34,7 +34,8 @@ def _units():
     units = [("api", "api.cu", []), ("plan", "plan.cu", []), ("gather", "gather.cu", []),
              ("noalloc", "noalloc.cu", []), ("robin", "robin.cu", []),
              ("select", "select.cu", []), ("postproc", "postproc.cu", ["-fmad=false"]),
-             ("coo", "coo.cu", ["-fmad=false"])]
+             ("coo", "coo.cu", []),
+             ("heat", "heat.cu", ["-fmad=false"])]
     for form in (0, 1, 2):
         for kind in (0, 1, 2):
             units.append((f"element_{form}_{kind}", "element_inst.cu", [f"-DEMG_FORM={form}", f"-DEMG_KIND={kind}"]))

@@ -21,7 +21,7 @@ import torch
 from scipy.sparse import csc_matrix
 
 from . import _lib as L
-from .assembly import _device, _to_dev
+from .assembly import _device, _prec, _to_dev
 
 __all__ = ["Legrange2", "CooValues", "GpuCOOMapping", "tet_stiffness_matrix", "tet_mass_matrix"]
 
@@ -38,24 +38,42 @@ class Legrange2:
 
 
 class CooValues:
-    """COO slot values on the device (f8 or c16 [S]); arithmetic between
-    values of the same slot layout stays on the device."""
+    """COO slot values on the device (f8 or c16): 100 per tet, either in the
+    reference's row-major blocks or (``transposed``, as the element kernels
+    write them for the gather) with each tet's block transposed. ``np.asarray``
+    gives the reference layout; arithmetic stays on the device."""
 
-    def __init__(self, values: torch.Tensor, layout):
+    def __init__(self, values: torch.Tensor, layout, transposed: bool = False):
         self.values = values
         self.layout = layout
+        self.transposed = bool(transposed)
 
     def __len__(self):
         return int(self.values.numel())
 
     def _wrap(self, v):
-        return CooValues(v, self.layout)
+        return CooValues(v, self.layout, self.transposed)
+
+    def _flip(self, v: torch.Tensor) -> torch.Tensor:
+        return v.view(-1, 10, 10).transpose(1, 2).reshape(-1)
+
+    def reference_layout(self) -> torch.Tensor:
+        """The values in the reference's slot order (device)."""
+        return self._flip(self.values) if self.transposed else self.values
 
     def _other(self, o):
         if isinstance(o, CooValues):
             if o.layout is not self.layout:
                 raise ValueError("COO values of different slot layouts")
-            return o.values
+            if o.transposed == self.transposed:
+                return o.values
+            return self._flip(o.values)
+        if isinstance(o, (np.ndarray, torch.Tensor)) and np.ndim(o) > 0:
+            t = o if isinstance(o, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(o))
+            t = t.to(self.values.device).reshape(-1)
+            if t.numel() != self.values.numel():
+                raise ValueError("COO arrays differ in length")
+            return self._flip(t) if self.transposed else t
         return o
 
     def __add__(self, o):
@@ -70,7 +88,7 @@ class CooValues:
         return self._wrap(self._other(o) - self.values)
 
     def __mul__(self, c):
-        if isinstance(c, CooValues):
+        if isinstance(c, CooValues) or np.ndim(c) > 0:
             raise TypeError("only scalar multiples of COO values")
         return self._wrap(self.values * c)
 
@@ -83,7 +101,7 @@ class CooValues:
         return self._wrap(-self.values)
 
     def __array__(self, dtype=None, copy=None):
-        a = self.values.cpu().numpy()
+        a = self.reference_layout().cpu().numpy()
         return a if dtype is None else a.astype(dtype)
 
 
@@ -101,6 +119,7 @@ class GpuCOOMapping:
         S = int(d_rows.numel())
         if d_cols.numel() != S:
             raise ValueError("rows and cols differ in length")
+        self.block_dofs = 0  # 10 when the slots are 10x10 blocks per tet (from_tet_to_field)
         m = L.CooMap()
         L.check(L.lib().emg_coo_init(S, self.N, L.ctypes.byref(m)))
         self.desc = m
@@ -108,7 +127,6 @@ class GpuCOOMapping:
         self._rows = d_rows.to(torch.int32).contiguous()
         cols = d_cols.to(torch.int32).contiguous()
         self.d_perm = torch.empty(m.perm_bytes // 4, dtype=torch.int32, device=dev)
-        self.d_run = torch.empty(m.run_bytes // 4, dtype=torch.int32, device=dev)
         ws = torch.empty(max(m.workspace_bytes, 1), dtype=torch.uint8, device=dev)
         self.d_indptr = torch.empty(self.N + 1, dtype=torch.int32, device=dev)
         status = torch.zeros(2, dtype=torch.int64, device=dev)
@@ -117,8 +135,10 @@ class GpuCOOMapping:
                                       L.ptr(ws), L.ptr(self.d_indptr), L.ptr(status), st))
         self.nnz = int(m.nnz)
         self.d_indices = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
+        self.d_run = torch.empty(self.nnz + 1, dtype=torch.int32, device=dev)
         L.check(L.lib().emg_coo_finish(L.ctypes.byref(m), L.ptr(self._rows), L.ptr(self.d_perm), L.ptr(ws),
                                        L.ptr(self.d_indptr), L.ptr(self.d_indices), L.ptr(self.d_run), st))
+        self._rows = None  # the rows live on in d_indices
         self._indptr = self._indices = None
 
     @staticmethod
@@ -143,7 +163,9 @@ class GpuCOOMapping:
         cols = torch.empty(max(S, 1), dtype=torch.int32, device=dev)
         L.check(L.lib().emg_coo_rowcol(L.ptr(d_t2f), int(D), int(nT), L.ptr(rows), L.ptr(cols),
                                        L.stream_handle(dev)))
-        return GpuCOOMapping(rows[:S], cols[:S], N)
+        cm = GpuCOOMapping(rows[:S], cols[:S], N)
+        cm.block_dofs = int(D)
+        return cm
 
     @property
     def indptr(self) -> np.ndarray:
@@ -159,8 +181,13 @@ class GpuCOOMapping:
 
     def to_device(self, data) -> torch.Tensor:
         """CSC values on the device (f8, or c16 for complex slot values)."""
+        block = 0
         if isinstance(data, CooValues):
             v = data.values
+            if data.transposed:
+                if self.block_dofs != 10:
+                    raise ValueError("transposed block values need a mapping of 10x10 element blocks")
+                block = 10
         elif isinstance(data, torch.Tensor):
             v = data
         else:
@@ -173,7 +200,8 @@ class GpuCOOMapping:
             raise ValueError(f"{v.numel()} slot values for a mapping of {self.S} slots")
         out = torch.empty(max(self.nnz, 1), dtype=v.dtype, device=self.device)
         L.check(L.lib().emg_coo_gather(L.ctypes.byref(self.desc), L.ptr(self.d_perm), L.ptr(self.d_run),
-                                       1 if cplx else 0, L.ptr(v), L.ptr(out), L.stream_handle(self.device)))
+                                       1 if cplx else 0, block, L.ptr(v), L.ptr(out),
+                                       L.stream_handle(self.device)))
         return out[: self.nnz]
 
     def to_csc(self, data) -> csc_matrix:
@@ -216,7 +244,10 @@ def _heat_mesh(field, device) -> _HeatMesh:
     return h[1]
 
 
-def _element(field, coef: np.ndarray, kind: int, device) -> tuple[CooValues, GpuCOOMapping]:
+def _element(field, coef: np.ndarray, kind: int, precision: str, device) -> tuple[CooValues, GpuCOOMapping]:
+    prec = _prec(precision)
+    if prec == L.EMG_MIXED:
+        raise ValueError("the heat elements come in 'fp64' (the reference's quadrature loop) and 'exact' (moments)")
     hm = _heat_mesh(field, device)
     dev = hm.nodes.device
     d_coef = _to_dev(np.ascontiguousarray(coef, dtype=np.float64), torch.float64, dev)
@@ -224,31 +255,37 @@ def _element(field, coef: np.ndarray, kind: int, device) -> tuple[CooValues, Gpu
     status = torch.zeros(2, dtype=torch.int64, device=dev)
     st = L.stream_handle(dev)
     L.check(L.lib().emg_leg2_element(L.ptr(hm.nodes), hm.n_nodes, L.ptr(hm.tets), hm.n_tets, L.ptr(d_coef), kind,
-                                     L.ptr(vals), L.ptr(status), st))
+                                     prec, L.EMG_LAYOUT_COO_T, L.ptr(vals), L.ptr(status), st))
     f, i = L.ctypes.c_int64(), L.ctypes.c_int64()
     L.check(L.lib().emg_status_read(L.ptr(status), L.ctypes.byref(f), L.ctypes.byref(i), st))
     if f.value:
         raise L.EmgMeshError(L.EMG_EMESH, f"tet {i.value}: "
                              + ("bad node index" if f.value & L.EMG_ST_INDEX else "degenerate tet"))
-    return CooValues(vals[: 100 * hm.n_tets], hm.cmap), hm.cmap
+    return CooValues(vals[: 100 * hm.n_tets], hm.cmap, transposed=True), hm.cmap
 
 
-def tet_stiffness_matrix(field, cond_termal: np.ndarray, *, device=None) -> tuple[CooValues, GpuCOOMapping]:
+def tet_stiffness_matrix(field, cond_termal: np.ndarray, *, precision: str = "fp64",
+                         device=None) -> tuple[CooValues, GpuCOOMapping]:
     """Drop-in for grad.py:403-437: the stiffness COO values
     K_ij = V sum_q w_q (k grad N_i) . grad N_j per tet (conductivity
-    f8[3, 3, n_tets]) and the COO -> CSC mapping."""
+    f8[3, 3, n_tets]) and the COO -> CSC mapping. ``precision``: 'fp64' runs
+    the reference's quadrature loop in its operation order; 'exact' folds the
+    same rule into 16 gradient products per tet (translation invariant; about
+    30x fewer operations)."""
     c = np.asarray(cond_termal, dtype=np.float64)
     nT = np.asarray(field.mesh.tets).shape[1]
     if c.shape != (3, 3, nT):
         raise ValueError(f"cond_termal must be (3, 3, {nT})")
-    return _element(field, c, 0, device)
+    return _element(field, c, 0, precision, device)
 
 
-def tet_mass_matrix(field, rho_cp: np.ndarray, *, device=None) -> tuple[CooValues, GpuCOOMapping]:
+def tet_mass_matrix(field, rho_cp: np.ndarray, *, precision: str = "fp64",
+                    device=None) -> tuple[CooValues, GpuCOOMapping]:
     """Drop-in for grad.py:440-462: the capacity COO values
-    M_ij = rho_cp V sum_q w_q N_i N_j per tet and the COO -> CSC mapping."""
+    M_ij = rho_cp V sum_q w_q N_i N_j per tet and the COO -> CSC mapping
+    ('exact': rho_cp V times the rule's constant 10x10 block)."""
     r = np.asarray(rho_cp, dtype=np.float64).ravel()
     nT = np.asarray(field.mesh.tets).shape[1]
     if r.shape != (nT,):
         raise ValueError(f"rho_cp must have {nT} values")
-    return _element(field, r, 1, device)
+    return _element(field, r, 1, precision, device)

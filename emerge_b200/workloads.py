@@ -188,3 +188,43 @@ def wr90_pml_slivers(n=(84, 50, 40), jitter=0.05, seed=4, freq=10e9, shell=0.10,
     wl = Workload("wr90_pml_slivers", f, er, ur, np.zeros(0, np.int64), freq, tuple(n))
     wl.slivers = pick
     return wl
+
+
+class HeatWorkload:
+    """A Lagrange-2 heat-conduction case: a jittered box, a random symmetric
+    positive-definite conductivity tensor and a rho_cp per tet."""
+
+    def __init__(self, name, field, cond, rho_cp, hex_grid):
+        self.name, self.field, self.cond, self.rho_cp, self.hex_grid = name, field, cond, rho_cp, hex_grid
+
+    @property
+    def n_tets(self) -> int:
+        return int(self.field.mesh.n_tets)
+
+
+def heat_box(n=(100, 50, 67), jitter=0.15, seed=6, size=(0.1, 0.05, 0.067)) -> HeatWorkload:
+    from .heat import Legrange2
+
+    nodes, tets = structured_box(*n, size=size, jitter=jitter, seed=seed)
+    m = TetMesh(nodes, tets)
+    rng = np.random.default_rng(seed)
+    nT = m.n_tets
+    cond = np.empty((3, 3, nT))
+    for lo in range(0, nT, 1 << 20):  # Q Q^T + 0.5 I, blockwise to bound host memory
+        hi = min(nT, lo + (1 << 20))
+        Q = rng.normal(size=(hi - lo, 3, 3))
+        cond[:, :, lo:hi] = np.einsum("nij,nkj->ikn", Q, Q) + 0.5 * np.eye(3)[:, :, None]
+    rho_cp = rng.uniform(1e6, 4e6, nT)
+    return HeatWorkload(f"heat_box_{nT // 1000}k", Legrange2(m), cond, rho_cp, tuple(n))
+
+
+def heat_element_alg_bytes(n_nodes: int, n_tets: int, kind: str) -> int:
+    """One Lagrange-2 element launch: node coordinates once, 4 node indices
+    and the material per tet (9 or 1 f8), 100 f8 values written."""
+    return 24 * n_nodes + n_tets * (16 + (72 if kind == "stiff" else 8) + 800)
+
+
+def heat_gather_alg_bytes(n_tets: int, nnz: int) -> int:
+    """One COO -> CSC gather: per slot its index (4 B) and value (8 B), per
+    entry its run start (4 B) read and its value (8 B) written."""
+    return n_tets * 100 * 12 + nnz * 12

@@ -91,6 +91,9 @@ enum {
                             value[ia*210 + x*(41-x)/2 + (y-x)], x <= y; the
                             assembly path's layout (each unique entry computed
                             once, half the bytes) */
+  EMG_LAYOUT_COO_T = 2,  /* D x D blocks per tet, transposed: value (i, j) of tet t
+                            at D^2 t + D j + i (the Lagrange-2 element values
+                            read by the COO gather with block_dofs = D) */
 };
 
 typedef struct {
@@ -358,8 +361,9 @@ int emg_port_overlap(const double *d_nodes, int64_t n_nodes, const int32_t *d_te
  * counted and scattered per column, each column's slots sorted by (row, slot)
  * (a fixed order), its distinct rows are its entries; an entry's value is the
  * sum of its slots in that order. Sizes from emg_coo_init: d_perm perm_bytes,
- * d_run run_bytes, workspace workspace_bytes (keep it from build to finish),
- * d_indptr N + 1, d_indices nnz (set by emg_coo_build, which synchronises). */
+ * workspace workspace_bytes (keep it from build to finish), d_indptr N + 1;
+ * then, with nnz set by emg_coo_build (which synchronises), d_indices nnz and
+ * d_run nnz + 1 int32 (run_bytes bounds it before nnz is known). */
 typedef struct {
   int64_t S, N, nnz;
   size_t perm_bytes, run_bytes, workspace_bytes;
@@ -374,16 +378,24 @@ int emg_coo_build(emg_coo_map *map, const int32_t *d_rows, const int32_t *d_cols
                   int32_t *d_indptr, int64_t *d_status, emg_stream_t stream);
 int emg_coo_finish(const emg_coo_map *map, const int32_t *d_rows, const int32_t *d_perm, void *d_workspace,
                    const int32_t *d_indptr, int32_t *d_indices, int32_t *d_run, emg_stream_t stream);
-/* CSC values (f64, or complex128 when is_complex) from slot values. */
-int emg_coo_gather(const emg_coo_map *map, const int32_t *d_perm, const int32_t *d_run, int is_complex,
+/* CSC values (f64, or complex128 when is_complex) from slot values:
+ * block_dofs 0 reads slot s at d_values[s]; block_dofs 10 reads values stored
+ * as transposed 10x10 blocks (EMG_LAYOUT_COO_T) of slots 100 t + 10 i + j. */
+int emg_coo_gather(const emg_coo_map *map, const int32_t *d_perm, const int32_t *d_run, int is_complex, int block_dofs,
                    const void *d_values, void *d_out, emg_stream_t stream);
 
 /* Heat conduction, Lagrange-2 (10 DoFs per tet): per tet the 10x10 block in
  * the reference's COO slots (row-major), kind 0 = stiffness with the
  * conductivity d_coef f64 [3][3][n_tets] (leg2_tet_stiff, grad.py:199-260),
- * kind 1 = mass with d_coef = rho_cp f64 [n_tets] (leg2_tet_mass :263-330). */
+ * kind 1 = mass with d_coef = rho_cp f64 [n_tets] (leg2_tet_mass :263-330).
+ * precision EMG_FP64: the reference's quadrature loop and operation order;
+ * EMG_EXACT: the same rule folded into per-tet moments (translation
+ * invariant, no cancellation in the barycentrics). layout EMG_LAYOUT_COO (the
+ * reference's row-major blocks) or EMG_LAYOUT_COO_T (transposed blocks). A
+ * degenerate tet or bad node index sets d_status and gets a zero block. */
 int emg_leg2_element(const double *d_nodes, int64_t n_nodes, const int32_t *d_tets, int64_t n_tets,
-                     const double *d_coef, int kind, double *d_values, int64_t *d_status, emg_stream_t stream);
+                     const double *d_coef, int kind, int precision, int layout, double *d_values, int64_t *d_status,
+                     emg_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,9 @@
  */
 #include <math.h>
 #include <stdint.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 static const double HEAT_DPTS[5][11] = {
     {-0.078933, 0.04573333, 0.04573333, 0.04573333, 0.04573333, 0.14933333, 0.14933333, 0.14933333, 0.14933333,
@@ -152,4 +155,18 @@ int oracle_leg2_builder(const double *nodes, int64_t nN, const int64_t *tets, in
     }
   }
   return 0;
+}
+
+/* scatter_to_csc_f8 (mth/csc_cast.py:150-177) for real data: the CSC value of
+ * each entry is the sum of its COO slots in the pattern's slot order */
+void oracle_scatter_f8(const double *data, const int64_t *perm, const int64_t *target, const int64_t *col_offsets,
+                       int64_t N, double *data_csc, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < N; ++i)
+    for (int64_t k = col_offsets[i]; k < col_offsets[i + 1]; ++k) data_csc[target[k]] += data[perm[k]];
 }

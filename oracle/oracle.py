@@ -63,6 +63,8 @@ def lib():
         L.oracle_csc_pattern.argtypes = [_p, _p, _i64, _i64, _p, _p, _p, _p, ctypes.c_int]
         L.oracle_csc_indices.restype = None
         L.oracle_csc_indices.argtypes = [_p, _p, _p, _i64, _p]
+        L.oracle_scatter_f8.restype = None
+        L.oracle_scatter_f8.argtypes = [_p, _p, _p, _p, _i64, _p, ctypes.c_int]
         L.oracle_scatter_c16.restype = None
         L.oracle_scatter_c16.argtypes = [_p, _p, _p, _p, _i64, _p, ctypes.c_int]
         L.oracle_scatter_lincomb_c16.restype = None
@@ -147,6 +149,14 @@ class CSCPattern:
         indices = np.empty(nnz, dtype=np.int64)
         lib().oracle_csc_indices(_ptr(rows), _ptr(perm), _ptr(target), S, _ptr(indices))
         return CSCPattern(indptr, indices, target, col_offsets, perm, N)
+
+    def values_f8(self, data, nthreads: int = 0) -> np.ndarray:
+        """``scatter_to_csc_f8`` (csc_cast.py:150-177): real data."""
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        out = np.zeros(self.nnz, dtype=np.float64)
+        lib().oracle_scatter_f8(_ptr(data), _ptr(self.perm), _ptr(self.target), _ptr(self.col_offsets), self.N,
+                                _ptr(out), int(nthreads))
+        return out
 
     def values(self, data, nthreads: int = 0) -> np.ndarray:
         data = np.ascontiguousarray(data, dtype=np.complex128)

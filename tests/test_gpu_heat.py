@@ -2,8 +2,8 @@
 the GPU, against the reference's own output (tests/golden/heat.npz) and the
 oracle. Tolerance 1e-12 relative (Frobenius and max entry) for values; the
 CSC pattern is bit-exact. At larger sizes: K annihilates constants (the
-Lagrange basis sums to one) and the entries of M sum to the integral of
-rho_cp."""
+Lagrange basis sums to one) and the entries of M sum to the quadrature's
+integral of rho_cp."""
 import numpy as np
 import pytest
 import torch
@@ -24,12 +24,13 @@ def heat_field():
     return Legrange2(TetMesh(nodes, tets))
 
 
-def test_heat_matrices_match_reference_golden():
+@pytest.mark.parametrize("precision", ["fp64", "exact"])
+def test_heat_matrices_match_reference_golden(precision):
     g = load_npz("heat.npz")
     f = heat_field()
     assert f.n_field == int(g["N"])
-    K, cmap = tet_stiffness_matrix(f, g["cond"])
-    M, cmap2 = tet_mass_matrix(f, g["rho_cp"])
+    K, cmap = tet_stiffness_matrix(f, g["cond"], precision=precision)
+    M, cmap2 = tet_mass_matrix(f, g["rho_cp"], precision=precision)
     assert cmap2 is cmap  # one resident mapping per field
     for mine, ref in ((np.asarray(K), g["K"]), (np.asarray(M), g["M"])):
         fro, mx = rel_err(mine, ref)
@@ -58,6 +59,38 @@ def test_transient_combination_and_oracle_mass():
     ref = pat.values(O.leg2_values(f.mesh, g["rho_cp"], "mass").astype(np.complex128)).real
     fro, mx = rel_err(cmap.to_csc(M).data, ref)
     assert fro <= TOL and mx <= TOL, (fro, mx)
+
+
+def test_layouts_and_oracle_arithmetic():
+    """Through the C ABI: the row-major (reference) and transposed element
+    layouts hold the same values, and gathering either (block_dofs 0 / 10)
+    gives bit-identical CSC values. The fp64 form repeats the reference's
+    operations: it agrees with the oracle's C restatement to rounding."""
+    g = load_npz("heat.npz")
+    f = heat_field()
+    K, cmap = tet_stiffness_matrix(f, g["cond"])
+    M, _ = tet_mass_matrix(f, g["rho_cp"])
+    from emerge_b200.heat import _heat_mesh
+
+    hm = _heat_mesh(f, cmap.device)
+    st = L.stream_handle(cmap.device)
+    status = torch.zeros(2, dtype=torch.int64, device=cmap.device)
+    for kind, coef, vals in ((0, g["cond"], K), (1, g["rho_cp"], M)):
+        d_coef = torch.from_numpy(np.ascontiguousarray(coef)).cuda()
+        row = torch.empty(100 * hm.n_tets, dtype=torch.float64, device=cmap.device)
+        L.check(L.lib().emg_leg2_element(L.ptr(hm.nodes), hm.n_nodes, L.ptr(hm.tets), hm.n_tets, L.ptr(d_coef), kind,
+                                         L.EMG_FP64, L.EMG_LAYOUT_COO, L.ptr(row), L.ptr(status), st))
+        assert torch.equal(row, vals.reference_layout())
+        a = torch.empty(cmap.nnz, dtype=torch.float64, device=cmap.device)
+        L.check(L.lib().emg_coo_gather(L.ctypes.byref(cmap.desc), L.ptr(cmap.d_perm), L.ptr(cmap.d_run), 0, 0,
+                                       L.ptr(row), L.ptr(a), st))
+        assert torch.equal(a, cmap.to_device(vals))
+        ref = O.leg2_values(f.mesh, coef, "stiff" if kind == 0 else "mass")
+        assert rel_err(row.cpu().numpy(), ref)[1] <= 1e-14
+    assert int(status[0]) == 0
+    # mixing layouts: a host array in the reference layout joins device values
+    A = cmap.to_csc(K + g["M"])
+    assert rel_err(A.data, cmap.to_csc(K).data + cmap.to_csc(M).data)[1] <= 1e-14
 
 
 @pytest.mark.parametrize("cplx", [False, True])
@@ -116,14 +149,35 @@ def test_degenerate_tet_raises():
     bad = Legrange2.__new__(Legrange2)
     bad.mesh = type("M", (), {"nodes": m.nodes, "tets": tets, "n_nodes": m.n_nodes, "n_edges": m.n_edges})()
     bad.tet_to_field, bad.n_field = f.tet_to_field, f.n_field
-    with pytest.raises(L.EmgMeshError):
-        tet_mass_matrix(bad, np.ones(m.n_tets))
+    for precision in ("fp64", "exact"):
+        with pytest.raises(L.EmgMeshError, match="degenerate"):
+            tet_mass_matrix(bad, np.ones(m.n_tets), precision=precision)
+        with pytest.raises(L.EmgMeshError, match="degenerate"):
+            tet_stiffness_matrix(bad, np.ones((3, 3, m.n_tets)), precision=precision)
 
 
-def test_properties_at_size():
+def test_exact_form_is_translation_invariant():
+    """The moment form does not depend on where the mesh sits: shifting the
+    box by 1e3 of its own size changes its values by rounding only, while the
+    two forms still agree to 1e-12 at the origin."""
+    g = load_npz("heat.npz")
+    f = heat_field()
+    K0 = np.asarray(tet_stiffness_matrix(f, g["cond"], precision="exact")[0])
+    Kf = np.asarray(tet_stiffness_matrix(f, g["cond"], precision="fp64")[0])
+    assert rel_err(K0, Kf)[1] <= 1e-12
+    shifted = Legrange2(TetMesh(f.mesh.nodes + 50.0, f.mesh.tets))
+    K1 = np.asarray(tet_stiffness_matrix(shifted, g["cond"], precision="exact")[0])
+    assert rel_err(K1, K0)[1] <= 1e-11
+    with pytest.raises(ValueError):
+        tet_mass_matrix(f, g["rho_cp"], precision="mixed")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "exact"])
+def test_properties_at_size(precision):
     """A 192k-tet box: K @ 1 = 0 (gradients of a constant vanish) and the
-    entries of M sum to sum_t rho_cp V_t (the basis is a partition of
-    unity); the pattern has one column per DoF with the diagonal in it."""
+    entries of M sum to sum_q w_q * sum_t rho_cp V_t (the basis is a
+    partition of unity; the reference's 8-digit weights sum to 1.0000003, not
+    1); the pattern has one column per DoF with the diagonal in it."""
     nodes, tets = structured_box(40, 20, 40, jitter=0.15, seed=4)
     m = TetMesh(nodes, tets)
     f = Legrange2(m)
@@ -131,15 +185,17 @@ def test_properties_at_size():
     Q = rng.normal(size=(m.n_tets, 3, 3))
     cond = np.einsum("nij,nkj->ikn", Q, Q) + 0.5 * np.eye(3)[:, :, None]
     rho = rng.uniform(1.0, 3.0, m.n_tets)
-    K, cmap = tet_stiffness_matrix(f, cond)
-    M, _ = tet_mass_matrix(f, rho)
+    K, cmap = tet_stiffness_matrix(f, cond, precision=precision)
+    M, _ = tet_mass_matrix(f, rho, precision=precision)
     A = cmap.to_csc(K)
     one = np.ones(f.n_field)
     assert np.abs(A @ one).max() <= 1e-9 * np.abs(A.data).max()
     X = m.nodes[:, m.tets]  # (3, 4, nT)
     V = np.abs(np.einsum("it,it->t", X[:, 1] - X[:, 0], np.cross(X[:, 2] - X[:, 0], X[:, 3] - X[:, 0], axis=0))) / 6
     Mc = cmap.to_device(M)
-    assert abs(float(Mc.sum()) - float((rho * V).sum())) <= 1e-10 * float((rho * V).sum())
+    wsum = -0.078933 + 4 * 0.04573333 + 6 * 0.14933333
+    expect = wsum * float((rho * V).sum())
+    assert abs(float(Mc.sum()) - expect) <= 1e-10 * expect
     assert np.all(np.diff(A.indptr) > 0)
     d = A.diagonal()
     assert np.all(d > 0)

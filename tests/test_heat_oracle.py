@@ -29,3 +29,4 @@ def test_leg2_values_and_pattern_match_reference():
     assert np.array_equal(pat.indptr, g["indptr"]) and np.array_equal(pat.indices, g["indices"])
     fro, mx = rel_err(pat.values(K.astype(np.complex128)).real, g["Kdata"])
     assert fro <= 1e-12 and mx <= 1e-12
+    assert np.array_equal(pat.values_f8(K), pat.values(K.astype(np.complex128)).real)
