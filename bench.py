@@ -631,16 +631,18 @@ def run_heat(args, rank, world, local_rank):
     hbm = peaks.get("hbm_gbs") or 6650.0
     src = "measured" if peaks.get("hbm_gbs") else "fallback"
 
-    def roof(r):
+    def roof(r, form):
         kb = {"k_leg2_stiff": W.heat_element_alg_bytes(nN, nT, "stiff"),
               "k_leg2_mass": W.heat_element_alg_bytes(nN, nT, "mass"), "k_coo_gather": W.heat_gather_alg_bytes(nT, nnz)}
         kms = {"k_leg2_stiff": r["k_stiff_ms"], "k_leg2_mass": r["k_mass_ms"], "k_coo_gather": r["k_gather_ms"]}
+        tr = load_traffic(wl.name) or {}
         kern = {k: {"alg_bytes": kb[k], "ms": kms[k], "achieved": kb[k] / (kms[k] * 1e-3) / 1e9,
-                    "frac": kb[k] / (kms[k] * 1e-3) / 1e9 / hbm} for k in kb}
+                    "frac": kb[k] / (kms[k] * 1e-3) / 1e9 / hbm, "traffic": tr.get(f"{form}_{k}_bytes")}
+                for k in kb}
         dom = max(kms, key=kms.get)
         d = kern[dom]
         return {"bound": "hbm", "kernel": dom, "achieved": d["achieved"], "peak": hbm, "unit": "GB/s",
-                "frac": d["frac"], "traffic": None, "peak_source": src, "alg_bytes_per_launch": d["alg_bytes"],
+                "frac": d["frac"], "traffic": d["traffic"], "peak_source": src, "alg_bytes_per_launch": d["alg_bytes"],
                 "kernels": kern}
 
     ex, fp = res["exact"], res["fp64"]
@@ -654,9 +656,9 @@ def run_heat(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}" if world > 1 else "1 gpu"},
             "plain_fp64": {"value": world * nT / (fp["ms"] * 1e-3), "ms_per_step": fp["ms"],
                            "k_stiff_ms": fp["k_stiff_ms"], "k_mass_ms": fp["k_mass_ms"],
-                           "note": "the reference's quadrature loop: FP64-arithmetic bound"},
+                           "note": "the reference's quadrature loop: FP64-issue bound", "roofline": roof(fp, "fp64")},
             "kernels_ms": {k: v for k, v in ex.items() if k != "ms"}, "exact_vs_fp64_max_rel": form_diff,
-            "roofline": roof(ex), "clocks": sampler.summary(), "e2e": e2e, "gpu_launches": 4 * args.steps}
+            "roofline": roof(ex, "exact"), "clocks": sampler.summary(), "e2e": e2e, "gpu_launches": 4 * args.steps}
     return line, wl
 
 
