@@ -89,7 +89,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "10"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
@@ -100,6 +100,19 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def preroll(self, step, min_samples: int = 5, max_s: float = 1.5):
+        """Untimed steps, right before the timed ones, until the sampler has
+        min_samples readings under this load (nvidia-smi reads every 50 ms
+        at best, so a timed region of tens of ms alone would give one)."""
+        import torch
+
+        if self.proc is None:
+            return
+        n0, t0 = len(self.lines), time.perf_counter()
+        while len(self.lines) - n0 < min_samples and time.perf_counter() - t0 < max_s:
+            step()
+            torch.cuda.synchronize()
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -126,7 +139,8 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "window": "untimed pre-roll steps, warm-up and timed steps of the same workload"}
 
 
 # ---------------------------------------------------------------- CPU baseline (oracle port)
@@ -291,6 +305,7 @@ def run_ours(args, rank, world, local_rank):
         sampler = ClockSampler(local_rank) if pname == "mixed" else None
         if sampler:
             sampler.__enter__()
+            sampler.preroll(step)
         ms = time_steps(step, args.steps, args.warmup, stream)
         if sampler:
             sampler.__exit__()
@@ -587,6 +602,7 @@ def run_heat(args, rank, world, local_rank):
 
         if pname == "exact":
             sampler.__enter__()
+            sampler.preroll(step)
         ms = time_steps(step, args.steps, args.warmup, stream)
         if pname == "exact":
             sampler.__exit__()
