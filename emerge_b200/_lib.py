@@ -21,7 +21,7 @@ EMG_LAYOUT_COO, EMG_LAYOUT_PACKED, EMG_LAYOUT_COO_T = 0, 1, 2
 
 # every symbol include/emgpu.h declares
 EXPORTS = (
-    "emg_version", "emg_last_error", "emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init",
+    "emg_version", "emg_last_error", "emg_device_check", "emg_material_classify", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
     "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
@@ -103,6 +103,8 @@ def lib():
     L.emg_last_error.restype = ctypes.c_char_p
     L.emg_device_check.argtypes = [ctypes.c_int]
     L.emg_status_reset.argtypes = [_P, _P]
+    L.emg_material_classify.argtypes = [_P, _I64, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]
     L.emg_status_read.argtypes = [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P]
     L.emg_plan_init.argtypes = [_I64, _I64, _I64, _I64, ctypes.POINTER(Plan)]
     L.emg_plan_build.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _P, _P, _P, _P, _P, _P]
@@ -140,7 +142,7 @@ def lib():
                                   _P]
     L.emg_assemble_noalloc.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
                                        ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
-    for name in ("emg_device_check", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
+    for name in ("emg_device_check", "emg_material_classify", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
                  "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",

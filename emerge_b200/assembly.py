@@ -78,7 +78,7 @@ def _prec(precision: str) -> int:
 class DeviceMesh:
     """Device copies of the mesh arrays the path reads (int32 SoA)."""
 
-    def __init__(self, field, conductor_tets=None, device=None, alloc=None):
+    def __init__(self, field, conductor_tets=None, device=None, alloc=None, reuse: "DeviceMesh | None" = None):
         dev = _device(device)
         mesh = field.mesh
         self.device = dev
@@ -94,7 +94,14 @@ class DeviceMesh:
         if dc.shape != (20,) or not np.array_equal(dc, [64] * 6 + [66] * 6 + [128] * 4 + [129] * 4):
             raise ValueError(f"unsupported dofcodes {dc.tolist()} (expected SECOND_MIXED_VOLAKIS)")
         self.nodes = _to_dev(mesh.nodes, torch.float64, dev, alloc)
-        self.tets = _to_dev(mesh.tets, torch.int32, dev, alloc)
+        # the device tets of ``reuse`` (a mapping's own mesh) when the caller
+        # passes the very same tet array again, as the reference does with its
+        # cached CSCMapping on every frequency; coordinates are always copied
+        if (reuse is not None and reuse._field.mesh.tets is mesh.tets and reuse.device == dev
+                and reuse.n_tets == self.n_tets):
+            self.tets = reuse.tets
+        else:
+            self.tets = _to_dev(mesh.tets, torch.int32, dev, alloc)
         self.tetids_host = _tet_assy(self.n_tets, conductor_tets)
         self.n_assy = int(self.tetids_host.shape[0]) if self.tetids_host is not None else self.n_tets
         self.tetids = _to_dev(self.tetids_host, torch.int32, dev, alloc) if self.tetids_host is not None else None
@@ -152,6 +159,16 @@ def _is_identity(t: np.ndarray) -> bool:
     return (all(not np.any(t[i, j] != 0) for i, j in off) and all(np.all(t[d, d] == 1) for d in range(3)))
 
 
+def material_kind(t: np.ndarray) -> tuple:
+    """(``classify_material(t)``, ``_is_identity(t)``) in one multi-threaded
+    native pass (emg_material_classify); t is c16[3, 3, nT]."""
+    a = np.ascontiguousarray(t, dtype=np.complex128)
+    k, i = L.ctypes.c_int(), L.ctypes.c_int()
+    L.check(L.lib().emg_material_classify(a.ctypes.data_as(L.ctypes.c_void_p), int(a.shape[2]), 0,
+                                          L.ctypes.byref(k), L.ctypes.byref(i)))
+    return int(k.value), bool(i.value)
+
+
 class DeviceMaterial:
     """Per-tet er, ur in the compact layout of their kind (see emg_material)."""
 
@@ -160,10 +177,10 @@ class DeviceMaterial:
         ur = np.asarray(ur)
         if er.shape != (3, 3, n_tets) or ur.shape != (3, 3, n_tets):
             raise ValueError(f"er/ur must have shape (3, 3, {n_tets})")
-        ur_id = _is_identity(ur)
-        kind = classify_material(er)
+        kind, _ = material_kind(er)
+        ur_kind, ur_id = material_kind(ur)
         if not ur_id:
-            kind = max(kind, classify_material(ur))
+            kind = max(kind, ur_kind)
         self.kind = kind
 
         def pack(t):
@@ -360,6 +377,7 @@ class GpuCSCMapping:
         del ws
         m.check_status()
         self._indptr = self._indices = None
+        self.dmesh = m  # its device tets are shared with later calls on the same tet array
         self._ws = None
         self._ws_prec = None
 
@@ -458,7 +476,7 @@ def tet_mass_stiffness_matrices(field, er: np.ndarray, ur: np.ndarray, conductor
     """Drop-in for curlcurl.py:222-270. Returns (dataE, dataB, cscmap) where
     dataE (stiffness) and dataB (mass) are lazy device-backed element values
     and cscmap is a ``GpuCSCMapping`` (built on first use, reused after)."""
-    dmesh = DeviceMesh(field, conductor_tets, device)
+    dmesh = DeviceMesh(field, conductor_tets, device, reuse=getattr(cscmap, "dmesh", None))
     dmat = DeviceMaterial(er, ur, dmesh.n_tets, dmesh.device)
     job = _Job(dmesh, dmat, _prec(precision))
     if cscmap is None:

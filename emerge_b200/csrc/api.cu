@@ -1,6 +1,10 @@
 // api.cu -- the extern "C" boundary of libemgpu (declared in include/emgpu.h).
 #include "common.cuh"
 
+#include <algorithm>
+#include <thread>
+#include <vector>
+
 namespace emg {
 
 namespace {
@@ -48,6 +52,58 @@ extern "C" {
 int emg_version(void) { return EMG_VERSION; }
 
 const char *emg_last_error(void) { return emg::last_error(); }
+
+// One pass over a complex128 [3][3][nT] tensor array on host threads: is any
+// off-diagonal entry nonzero (FULL), are the three diagonals equal tet by
+// tet (ISO, else DIAG), and is it the identity. Comparisons are numpy's for
+// complex values: nonzero when either part is, equal when both parts are
+// (a NaN is nonzero and equal to nothing).
+int emg_material_classify(const double *h_t, int64_t n_tets, int n_threads, int *h_kind, int *h_identity) {
+  if (!h_kind || !h_identity) return fail(EMG_EINVAL, "null output pointer");
+  if (n_tets < 0) return fail(EMG_EINVAL, "negative size");
+  if (n_tets > 0 && !h_t) return fail(EMG_EINVAL, "null tensor pointer");
+  const int64_t nT = n_tets;
+  int nth = n_threads > 0 ? n_threads : (int)std::thread::hardware_concurrency();
+  nth = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(nth, 1), nT / 65536));
+  struct Flags {
+    bool off = false, diag_ne = false, not_one = false;
+  };
+  std::vector<Flags> fl(nth);
+  auto work = [&](int w) {
+    const int64_t b = nT * w / nth, e = nT * (w + 1) / nth;
+    Flags f;
+    for (int c = 0; c < 9 && !f.off; ++c) {
+      if (c % 4 == 0) continue;  // diagonal component
+      const double *p = h_t + 2 * (int64_t)c * nT;
+      for (int64_t t = b; t < e; ++t)
+        if (p[2 * t] != 0.0 || p[2 * t + 1] != 0.0) {
+          f.off = true;
+          break;
+        }
+    }
+    const double *d0 = h_t, *d1 = h_t + 2 * 4 * nT, *d2 = h_t + 2 * 8 * nT;
+    for (int64_t t = b; t < e; ++t) {
+      const double a0 = d0[2 * t], b0 = d0[2 * t + 1], a1 = d1[2 * t], b1 = d1[2 * t + 1];
+      const double a2 = d2[2 * t], b2 = d2[2 * t + 1];
+      f.diag_ne |= !(a0 == a1 && b0 == b1 && a1 == a2 && b1 == b2);
+      f.not_one |= !(a0 == 1.0 && b0 == 0.0 && a1 == 1.0 && b1 == 0.0 && a2 == 1.0 && b2 == 0.0);
+    }
+    fl[w] = f;
+  };
+  std::vector<std::thread> pool;
+  for (int w = 1; w < nth; ++w) pool.emplace_back(work, w);
+  work(0);
+  for (auto &th : pool) th.join();
+  bool off = false, diag_ne = false, not_one = false;
+  for (const Flags &f : fl) {
+    off |= f.off;
+    diag_ne |= f.diag_ne;
+    not_one |= f.not_one;
+  }
+  *h_kind = off ? EMG_MAT_FULL : (diag_ne ? EMG_MAT_DIAG : EMG_MAT_ISO);
+  *h_identity = (!off && !not_one) ? 1 : 0;
+  return EMG_OK;
+}
 
 int emg_device_check(int device) {
   cudaDeviceProp p;

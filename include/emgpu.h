@@ -131,6 +131,14 @@ const char *emg_last_error(void);
  * on it. Replaces nothing in the reference (it has no GPU path). */
 int emg_device_check(int device);
 
+/* Host-only, multi-threaded: the material kind of a complex128 [3][3][nT]
+ * tensor array h_t (host memory, C order; the reference's er / ur layout,
+ * curlcurl.py:222-235) -- EMG_MAT_FULL if any off-diagonal entry is nonzero,
+ * else EMG_MAT_ISO if the three diagonals agree tet by tet, else EMG_MAT_DIAG --
+ * and whether it is the identity (*h_identity = 1). n_threads <= 0: all host
+ * threads. Lets the caller upload only the compact layout of emg_material. */
+int emg_material_classify(const double *h_t, int64_t n_tets, int n_threads, int *h_kind, int *h_identity);
+
 /* Status word helpers (d_status: int64[2] device memory). */
 int emg_status_reset(int64_t *d_status, emg_stream_t stream);
 int emg_status_read(const int64_t *d_status, int64_t *h_flags, int64_t *h_first_index, emg_stream_t stream);

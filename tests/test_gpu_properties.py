@@ -152,3 +152,23 @@ def test_chunk_order_changes_no_value(mid_case, precision):
         assert np.array_equal(outs[0], o)
     with pytest.raises(ValueError):
         GpuCSCMapping(dm, chunk_order="hilbert")
+
+
+def test_repeat_calls_share_device_tets_and_see_moved_nodes():
+    """A call that passes the mapping back with the same tet array reuses the
+    mapping's device tets (the reference's cached-CSCMapping call pattern);
+    node coordinates are copied every call, so moving nodes in place changes
+    the values exactly as a fresh assembly does."""
+    nodes, tets = structured_box(6, 4, 5, jitter=0.1, seed=2)
+    f = Nedelec2Field(TetMesh(nodes, tets))
+    er, ur = _blocky(f.ntets, np.random.default_rng(2))
+    E, B, cmap = tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64))
+    A1 = cmap.to_csc(E - B * 3.0).data
+    E2, B2, cmap2 = tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64), cmap)
+    assert cmap2 is cmap and E2.job.mesh.tets.data_ptr() == cmap.dmesh.tets.data_ptr()
+    assert np.array_equal(cmap.to_csc(E2 - B2 * 3.0).data, A1)
+    f.mesh.nodes[:, :] *= 1.5  # same topology, new geometry
+    E3, B3, _ = tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64), cmap)
+    E4, B4, c4 = tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64))
+    A3, A4 = cmap.to_csc(E3 - B3 * 3.0).data, c4.to_csc(E4 - B4 * 3.0).data
+    assert np.array_equal(A3, A4) and not np.array_equal(A3, A1)
