@@ -755,12 +755,16 @@ template <int FORM, int KIND, int LAYOUT>
 int launch_element_t(const ElemArgs &a, cudaStream_t s) {
   using ST = typename StoreT<typename FormReal<FORM>::T>::T;
   constexpr size_t smem = (size_t)ELEM_WARPS * 32 * 20 * sizeof(ST);
-  static bool configured = false;  // benign race: every thread sets the same value
-  if (!configured) {
+  // the attribute belongs to the current device: set once per device (benign
+  // race: every thread that gets here sets the same value)
+  static bool configured[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+  if (dev >= 64 || !configured[dev]) {
     cudaError_t e = cudaFuncSetAttribute(k_element<FORM, KIND, LAYOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return fail(EMG_ECUDA, "cudaFuncSetAttribute(k_element): %s", cudaGetErrorString(e));
-    configured = true;
+    if (dev < 64) configured[dev] = true;
   }
   if (a.nA == 0) return EMG_OK;
   k_element<FORM, KIND, LAYOUT><<<grid_for(a.nA, ELEM_THREADS), ELEM_THREADS, smem, s>>>(a);

@@ -476,14 +476,18 @@ extern "C" int emg_leg2_element(const double *d_nodes, int64_t n_nodes, const in
                                                         d_values, d_status);
     return launch_check("k_leg2_exact");
   }
-  static const bool carveout = [] {
-    cudaFuncSetAttribute(k_leg2_stiff_fp64, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    cudaFuncSetAttribute(k_leg2_mass_fp64, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    return true;
-  }();
-  (void)carveout;
+  // prefer shared memory over L1 for the fp64 kernels, once per device (a
+  // hint: a failure only costs occupancy, so its status is not an error)
+  static bool carveout[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !carveout[dev]) {
+    if (cudaFuncSetAttribute(k_leg2_stiff_fp64, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+        cudaFuncSetAttribute(k_leg2_mass_fp64, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      (void)cudaGetLastError();  // leave no error behind for the launch check
+    carveout[dev] = true;
+  }
   const int64_t blocks = (n_tets + kFp64Tets - 1) / kFp64Tets;
   if (kind == 0) {
     k_leg2_stiff_fp64<<<(unsigned)blocks, kFp64Threads, 0, s>>>(d_nodes, n_nodes, d_tets, n_tets, d_coef, tr,
