@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--sweep", action="store_true",
                     help="resident frequency sweep: 201 frequencies 8-12 GHz with the two port terms on the workload")
     ap.add_argument("--sweep-freqs", type=int, default=201)
-    ap.add_argument("--sweep-batch", type=int, default=8, help="frequencies formed per launch (outputs resident)")
+    ap.add_argument("--sweep-batch", type=int, default=12, help="frequencies formed per launch (outputs resident; 12 x 8.9 GB)")
     ap.add_argument("--pml", action="store_true",
                     help="anisotropic PML shell + 2%% slivers (1,008,000 tets): speed and mixed-vs-FP64 errors")
     ap.add_argument("--shard", action="store_true",
