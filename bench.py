@@ -82,7 +82,10 @@ class ClockSampler:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+        # nvidia-smi numbers GPUs physically; map a visible-device index
+        # through CUDA_VISIBLE_DEVICES when that restricts the visible set
+        vis = [x.strip() for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+        self.gpu = vis[gpu_index] if 0 <= gpu_index < len(vis) else str(gpu_index)
         self.proc = None
         self.lines = []
 
