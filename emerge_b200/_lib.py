@@ -26,7 +26,7 @@ EXPORTS = (
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
     "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
     "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values", "emg_ned2_interp",
-    "emg_port_overlap", "emg_coo_init", "emg_coo_rowcol", "emg_coo_build", "emg_coo_finish", "emg_coo_gather",
+    "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol", "emg_coo_build", "emg_coo_finish", "emg_coo_gather",
     "emg_leg2_element",
 )
 
@@ -132,6 +132,8 @@ def lib():
     L.emg_ned2_interp.argtypes = [_P, _I64, _P, _I64, _P, _P, _I64, _I64, _P, _P, _I64, _P, _P, _P]
     L.emg_port_overlap.argtypes = [_P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, ctypes.c_int, _P,
                                    _D, _P, _P, _P, _P]
+    L.emg_sparse_solve.argtypes = [_I64, _I64, _P, _P, _P, _P, _P, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_I64),
+                                   _P]
     L.emg_coo_init.argtypes = [_I64, _I64, ctypes.POINTER(CooMap)]
     L.emg_coo_rowcol.argtypes = [_P, ctypes.c_int, _I64, _P, _P, _P]
     L.emg_coo_build.argtypes = [ctypes.POINTER(CooMap), _P, _P, _P, _P, _P, _P, _P]
@@ -146,7 +148,7 @@ def lib():
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
                  "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
-                 "emg_select_values", "emg_ned2_interp", "emg_port_overlap", "emg_coo_init", "emg_coo_rowcol",
+                 "emg_select_values", "emg_ned2_interp", "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol",
                  "emg_coo_build", "emg_coo_finish", "emg_coo_gather", "emg_leg2_element"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L

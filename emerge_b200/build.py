@@ -34,7 +34,7 @@ def _units():
     units = [("api", "api.cu", []), ("plan", "plan.cu", []), ("gather", "gather.cu", []),
              ("noalloc", "noalloc.cu", []), ("robin", "robin.cu", []),
              ("select", "select.cu", []), ("postproc", "postproc.cu", ["-fmad=false"]),
-             ("coo", "coo.cu", []),
+             ("coo", "coo.cu", []), ("solve", "solve.cu", []),
              ("heat", "heat.cu", ["-fmad=false"])]
     for form in (0, 1, 2):
         for kind in (0, 1, 2):

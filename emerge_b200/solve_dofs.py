@@ -9,9 +9,14 @@ are not fixed by PEC conditions (solver.py:2071)::
 ``SolveSubmatrix(cscmap, solve_ids)`` builds the reduced pattern once (rows
 renumbered and ascending, as scipy's slicing gives them) and a map from each
 kept entry to its position in A; per frequency ``values(A)`` gathers the
-reduced values on the device, so a GPU solver never needs A on the host.
+reduced values on the device, so a GPU solver never needs A on the host;
+``solve`` hands them to a sparse direct solver on the device (cuSOLVER's
+sparse QR through emg_sparse_solve: the reference's cuDSS is not part of
+this toolkit) and ``expand`` puts the solution back on all N DoFs.
 """
 from __future__ import annotations
+
+import warnings
 
 import numpy as np
 import torch
@@ -77,3 +82,47 @@ class SolveSubmatrix:
         v = self.values(A).cpu().numpy()
         return csc_matrix((v, self.d_indices[: self.nnz].cpu().numpy(), self.d_indptr[: self.M + 1].cpu().numpy()),
                           shape=(self.M, self.M))
+
+    _REORDER = {"none": 0, "symrcm": 1, "symamd": 2, "metis": 3}
+
+    def solve(self, values: torch.Tensor, b: torch.Tensor, *, symmetric: bool = True, tol: float = 1e-12,
+              reorder: str = "symrcm") -> torch.Tensor:
+        """x (complex128 [M], device) with Asel x = b: ``values`` are Asel's
+        (``values(A)``), ``b`` the reduced right-hand side (``rhs``). With
+        ``symmetric`` (Asel = Asel^T, as for every system this library
+        assembles, port terms included) the CSC arrays are passed as CSR;
+        otherwise they are converted on the device first. Raises
+        np.linalg.LinAlgError if the solver finds Asel singular."""
+        dev = self.cmap.device
+        if self.M == 0:
+            return torch.zeros(0, dtype=torch.complex128, device=dev)
+        v = values.to(device=dev, dtype=torch.complex128).contiguous()[: self.nnz]
+        rhs = b.to(device=dev, dtype=torch.complex128).contiguous()
+        if v.numel() != self.nnz or rhs.numel() != self.M:
+            raise ValueError(f"values need {self.nnz} and b {self.M} entries")
+        if reorder not in self._REORDER:
+            raise ValueError(f"reorder must be one of {sorted(self._REORDER)}")
+        ptr, ind = self.d_indptr[: self.M + 1], self.d_indices[: self.nnz]
+        if not symmetric:  # CSC of Asel -> CSR of Asel (arrays from emg_select_*: valid by construction)
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore", UserWarning)
+                csr = torch.sparse_csc_tensor(ptr.to(torch.int64), ind.to(torch.int64), v, size=(self.M, self.M),
+                                              check_invariants=False).to_sparse_csr()
+            ptr = csr.crow_indices().to(torch.int32).contiguous()
+            ind = csr.col_indices().to(torch.int32).contiguous()
+            v = csr.values().contiguous()
+        x = torch.empty(self.M, dtype=torch.complex128, device=dev)
+        sing = L.ctypes.c_int64(-1)
+        L.check(L.lib().emg_sparse_solve(self.M, self.nnz, L.ptr(ptr), L.ptr(ind), L.ptr(v), L.ptr(rhs), L.ptr(x),
+                                         float(tol), self._REORDER[reorder], L.ctypes.byref(sing),
+                                         L.stream_handle(dev)))
+        if sing.value >= 0:
+            raise np.linalg.LinAlgError(f"the reduced system is singular (row {sing.value})")
+        return x
+
+    def expand(self, x: torch.Tensor) -> torch.Tensor:
+        """The solution on all N DoFs (complex128, device): x at solve_ids,
+        zero at the fixed (PEC) DoFs, as the reference's solution vector."""
+        full = torch.zeros(self.cmap.N, dtype=torch.complex128, device=self.cmap.device)
+        full[self.d_ids] = x.to(torch.complex128)
+        return full

@@ -363,6 +363,19 @@ int emg_port_overlap(const double *d_nodes, int64_t n_nodes, const int32_t *d_te
                      const double *h_rule, int nq, const void *d_U, double q, void *d_per_tri, void *d_total,
                      int64_t *d_status, emg_stream_t stream);
 
+/* Sparse direct solve of an n x n complex128 system on the device, the
+ * handoff after emg_select_*: A x = b with A in CSR (0-based, int32). The
+ * reference hands A[:, solve_ids][solve_ids, :] to SuperLU / Pardiso / MUMPS or
+ * to cuDSS (SolverCuDSS, solver.py:1274-1323; slicing :2071); cuDSS is not in
+ * this toolkit, so this calls cuSOLVER's sparse QR (cusolverSpZcsrlsvqr),
+ * loaded on first use (EMG_EDEVICE if it cannot be). The CSC arrays of a
+ * symmetric matrix (A = A^T, as every system this library assembles) are its
+ * CSR arrays. tol: singularity threshold; reorder: 0 none, 1 symrcm, 2 symamd,
+ * 3 metis (passed through). *h_singularity = -1 if A is invertible, else the
+ * first row found dependent. Blocking; cuSOLVER allocates its own scratch. */
+int emg_sparse_solve(int64_t n, int64_t nnz, const int32_t *d_row_ptr, const int32_t *d_col_ind, const void *d_values,
+                     const void *d_b, void *d_x, double tol, int reorder, int64_t *h_singularity, emg_stream_t stream);
+
 /* General COO -> CSC mapping: CSCMapping.from_rowcol / to_csc
  * (mth/csc_cast.py:51-177) for any slot list, as the heat-conduction assembly
  * uses it (physics/heatconduction/assembly/grad.py:403-460). Slots are

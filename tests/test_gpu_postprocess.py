@@ -103,3 +103,47 @@ def test_te10_guide_s_parameters_known_answer():
     S21r = (O.port_overlap(f, xr, p2, po2.tri_tets, TRI_RULE_6, U2, 0.0)[0]
             / O.port_overlap(f, z0, p2, po2.tri_tets, TRI_RULE_6, U2, -1.0)[0])
     assert abs(S21 - S21r) <= 1e-9 and abs(S11 - S11r) <= 1e-9, (S21, S21r, S11, S11r)
+
+
+def test_te10_known_answer_with_the_solve_on_the_gpu():
+    """The same guide with nothing on the host between the mesh and the
+    S-parameters: the reduced system is solved on the device
+    (SolveSubmatrix.solve), the solution expanded on the device. S21 =
+    exp(-j beta L), S11 = 0 as in the host-solve chain."""
+    import torch
+
+    from emerge_b200.assembly import tet_mass_stiffness_matrices
+    from emerge_b200.mesh import plane_tris
+    from emerge_b200.robin import RobinTerm
+    from emerge_b200.solve_dofs import SolveSubmatrix
+
+    wl = W.wr90_air(n=(6, 3, 15))
+    f = wl.field
+    m = f.mesh
+    a, b, length = W.WR90
+    k0, gamma = wl.k0, W.rect_port_gamma(wl.freq)
+    beta = abs(gamma)
+    p1, p2 = plane_tris(m, 2, 0.0), plane_tris(m, 2, float(m.nodes[2].max()))
+    walls = np.concatenate([plane_tris(m, ax, v) for ax, vals in ((0, (0.0, a)), (1, (0.0, b))) for v in vals])
+    solve = np.setdiff1d(np.arange(f.n_field), np.unique(f.tri_to_field[:, walls]))
+
+    def mode(P):
+        e = np.zeros(P.shape, np.complex128)
+        e[1] = np.sin(np.pi * P[0] / a)
+        return e
+
+    E, B, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    R1, R2 = RobinTerm(f, p1, cmap), RobinTerm(f, p2, cmap)
+    sub = SolveSubmatrix(cmap, solve)
+    Asel = sub.values(cmap.to_device(E - B * k0 ** 2 + (R1 + R2) * gamma))
+    bsel = sub.rhs(R1.force(-2j * beta * mode(R1.quadrature_points())))
+    x = sub.expand(sub.solve(Asel, bsel))
+    fod = FieldOnDevice(f)
+    po1, po2 = PortOverlap(fod, p1), PortOverlap(fod, p2)
+    U1, U2 = mode(po1.quadrature_points()), mode(po2.quadrature_points())
+    zero = torch.zeros_like(x)
+    S11 = po1(x, U1, 1.0)[0] / po1(zero, U1, -1.0)[0]
+    S21 = po2(x, U2, 0.0)[0] / po2(zero, U2, -1.0)[0]
+    assert abs(S11) < 1e-3, S11
+    assert abs(abs(S21) - 1) < 1e-3, S21
+    assert abs(np.angle(S21 / np.exp(-1j * beta * length))) < 5e-3, S21
