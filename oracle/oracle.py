@@ -73,6 +73,10 @@ def lib():
         L.oracle_num_threads.restype = ctypes.c_int
         L.oracle_tri_stiff.restype = None
         L.oracle_tri_stiff.argtypes = [_p, ctypes.c_double, ctypes.c_double, _p]
+        L.oracle_abc2_block.restype = None
+        L.oracle_abc2_block.argtypes = [_p, ctypes.c_double, ctypes.c_double, _p]
+        L.oracle_abc2_entries.restype = ctypes.c_int
+        L.oracle_abc2_entries.argtypes = [_p, _i64, _p, _i64, _p, _i64, ctypes.c_double, ctypes.c_double, _p]
         L.oracle_robin_entries.restype = ctypes.c_int
         L.oracle_robin_entries.argtypes = [_p, _i64, _p, _i64, _p, _i64, ctypes.c_double, ctypes.c_double, _p]
         L.oracle_tri_force.restype = None
@@ -234,6 +238,33 @@ def tri_stiff(X: np.ndarray, gamma: complex) -> np.ndarray:
     g = complex(gamma)
     lib().oracle_tri_stiff(_ptr(X), g.real, g.imag, _ptr(out))
     return out.reshape(8, 8)
+
+
+def abc2_block(X: np.ndarray, cf: complex) -> np.ndarray:
+    """``_abc_order_2_terms`` (robin_abc_order2.py:143-217): X f8[3, 3] ->
+    c16[8, 8], cf times the area-weighted curl-curl block."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.empty(64, np.complex128)
+    c = complex(cf)
+    lib().oracle_abc2_block(_ptr(X), c.real, c.imag, _ptr(out))
+    return out.reshape(8, 8)
+
+
+def abc2_entries(field, tri_ids, cf: complex, Mat: np.ndarray | None = None) -> np.ndarray:
+    """``abc_order_2_matrix`` / ``_matrix_builder`` (robin_abc_order2.py:225-281):
+    every listed tri's block added into the tri COO array c16[F*64]."""
+    m = field.mesh
+    F = m.tris.shape[1]
+    if Mat is None:
+        Mat = np.zeros(F * 64, np.complex128)
+    nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+    tris = np.ascontiguousarray(m.tris, dtype=np.int64)
+    ids = np.ascontiguousarray(tri_ids, dtype=np.int64)
+    c = complex(cf)
+    if lib().oracle_abc2_entries(_ptr(nodes), nodes.shape[1], _ptr(tris), F, _ptr(ids), ids.shape[0], c.real, c.imag,
+                                 _ptr(Mat)) != 0:
+        raise IndexError("triangle or node index out of range")
+    return Mat
 
 
 def robin_entries(field, tri_ids, gamma: complex, Bmat: np.ndarray | None = None) -> np.ndarray:

@@ -70,6 +70,8 @@ def load_reference(ref_root: str = DEFAULT_REF_ROOT):
     ns.ccbf = importlib.import_module("emerge._emerge.compiled.ccbf")
     # Robin boundary term (robinbc.py); imports cleanly with the stubs above
     ns.robinbc = importlib.import_module("emerge._emerge.physics.microwave.assembly.robinbc")
+    # second-order absorbing boundary correction (robin_abc_order2.py)
+    ns.abc2 = importlib.import_module("emerge._emerge.physics.microwave.assembly.robin_abc_order2")
     # post-processing: field interpolation and surface integrals
     if "emerge._emerge.compiled.base" not in sys.modules:
         _pkg("emerge._emerge.compiled.base", os.path.join(em, "compiled", "base"))

@@ -12,6 +12,11 @@
  *   ned2_tri_force / compute_force_entries       robinbc.py:220-313
  *   2-D basis functions _ne0_2d, _ne2_2d, _nf0_2d, _nf1_2d
  *                                                compiled/ccbf.py:81,107,269,284
+ *   second-order ABC correction _abc_order_2_terms / _matrix_builder
+ *                                physics/microwave/assembly/robin_abc_order2.py:143-251
+ *   its tri_coefficients and 6-point rule (14 digits)     robin_abc_order2.py:100-122, 89-98
+ *   2-D curls _curl_ne0_2d, _curl_ne2_2d, _curl_nf0_2d, _curl_nf1_2d
+ *                                                compiled/ccbf.py:168,178,386,397
  *
  * dofcodes2d of the Volakis set are [64, 64, 64, 66, 66, 66, 128, 129]
  * (elements/dofsets.py:39,114-115): three ne0 edge functions on the local
@@ -56,8 +61,9 @@ static void normalize3(double a[3]) {
  * (tri_coefficients) and the 8 Volakis functions at the 6 points.
  * X[d][v]: vertex v (0..2) coordinates. Returns the area; basis rows are
  * xhat, yhat, zhat. */
-static double tri_frame_basis(const double X[3][3], double basis[3][3], double f[8][2][6]) {
-  /* construct_local_vertices: origin at vertex 0, x along edge 0->1, z the normal */
+/* construct_local_vertices (robinbc.py:165-183): origin at vertex 0, x along
+ * edge 0->1, z the normal; the vertices' local coordinates tx, ty */
+static void tri_local(const double X[3][3], double basis[3][3], double tx[3], double ty[3]) {
   double e1[3], e2[3], xh[3], yh[3], zh[3];
   for (int d = 0; d < 3; ++d) {
     e1[d] = X[d][1] - X[d][0];
@@ -74,7 +80,6 @@ static double tri_frame_basis(const double X[3][3], double basis[3][3], double f
     basis[1][d] = yh[d];
     basis[2][d] = zh[d];
   }
-  double tx[3], ty[3];
   for (int v = 0; v < 3; ++v) {
     double rx = 0.0, ry = 0.0;
     for (int d = 0; d < 3; ++d) {
@@ -85,6 +90,11 @@ static double tri_frame_basis(const double X[3][3], double basis[3][3], double f
     tx[v] = rx;
     ty[v] = ry;
   }
+}
+
+static double tri_frame_basis(const double X[3][3], double basis[3][3], double f[8][2][6]) {
+  double tx[3], ty[3];
+  tri_local(X, basis, tx, ty);
   /* tri_coefficients */
   const double x1 = tx[0], x2 = tx[1], x3 = tx[2], y1 = ty[0], y2 = ty[1], y3 = ty[2];
   const double a[3] = {x2 * y3 - y2 * x3, x3 * y1 - y3 * x1, x1 * y2 - y1 * x2};
@@ -198,6 +208,90 @@ int oracle_force_entries(const double *nodes, int64_t nN, const int64_t *tris, i
     cplx bv[8];
     oracle_tri_force(X, Ui, bv);
     for (int k = 0; k < 8; ++k) b[t2f[k * F + t]] += bv[k];
+  }
+  return 0;
+}
+
+/* robin_abc_order2.py:89-98, its own copy of the rule: weights, L1..L3 */
+static const double ABC2_DPTS[4][6] = {
+    {0.10995174365532, 0.10995174365532, 0.10995174365532, 0.22338158967801, 0.22338158967801, 0.22338158967801},
+    {0.81684757298046, 0.09157621350977, 0.09157621350977, 0.10810301816807, 0.44594849091597, 0.44594849091597},
+    {0.09157621350977, 0.81684757298046, 0.09157621350977, 0.44594849091597, 0.10810301816807, 0.44594849091597},
+    {0.09157621350977, 0.09157621350977, 0.81684757298046, 0.44594849091597, 0.44594849091597, 0.10810301816807}};
+
+/* _abc_order_2_terms: B[a][b] = cf * A * sum_q w_q c_a(q) c_b(q) with c the
+ * scalar 2-D curls of the 8 functions in the triangle's plane. The reference
+ * also forms a divergence matrix, but writes the first function's divergence
+ * into the second function's buffer, which the inner loop overwrites before
+ * use, so that matrix is identically zero; it is left out here. */
+void oracle_abc2_block(const double X[3][3], double cf_re, double cf_im, cplx *out) {
+  double basis[3][3], tx[3], ty[3];
+  tri_local(X, basis, tx, ty);
+  const double x1 = tx[0], x2 = tx[1], x3 = tx[2], y1 = ty[0], y2 = ty[1], y3 = ty[2];
+  const double a[3] = {x2 * y3 - y2 * x3, x3 * y1 - y3 * x1, x1 * y2 - y1 * x2};
+  const double b[3] = {y2 - y3, y3 - y1, y1 - y2};
+  const double c[3] = {x3 - x2, x1 - x3, x2 - x1};
+  const double sA = 0.5 * ((x1 - x3) * (y2 - y1) - (x1 - x2) * (y3 - y1));
+  const double sign = sA > 0 ? 1.0 : (sA < 0 ? -1.0 : 0.0);
+  const double A = fabs(sA);
+  double ca[3], cb[3], cc[3];
+  for (int m = 0; m < 3; ++m) {
+    ca[m] = a[m] * sign / (2 * A);
+    cb[m] = b[m] * sign / (2 * A);
+    cc[m] = c[m] * sign / (2 * A);
+  }
+  static const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
+  double C[8][6];
+  for (int q = 0; q < 6; ++q) {
+    const double xs = x1 * ABC2_DPTS[1][q] + x2 * ABC2_DPTS[2][q] + x3 * ABC2_DPTS[3][q];
+    const double ys = y1 * ABC2_DPTS[1][q] + y2 * ABC2_DPTS[2][q] + y3 * ABC2_DPTS[3][q];
+    for (int e = 0; e < 3; ++e) {
+      const int i = EI[e], j = EJ[e];
+      const double ai = ca[i], bi = cb[i], ci = cc[i], aj = ca[j], bj = cb[j], cj = cc[j];
+      /* _curl_ne0_2d */
+      C[e][q] = 2 * bi * cj - 2 * bj * ci;
+      /* _curl_ne2_2d */
+      const double t0 = bj * xs, t1 = cj * ys, t2 = t0 + t1 + aj, t3 = ai + bi * xs + ci * ys;
+      C[3 + e][q] = -(bi - bj) * (t2 * ci - t3 * cj) + (ci - cj) * (t2 * bi - t3 * bj) +
+                    2 * (bi * cj - bj * ci) * (-t0 - t1 + t3 - aj);
+    }
+    {  /* _curl_nf0_2d on (0, 1, 2) */
+      const double t0 = ca[2] + cb[2] * xs + cc[2] * ys, t1 = ca[1] + cb[1] * xs + cc[1] * ys;
+      C[6][q] = -cb[0] * (t0 * cc[1] - t1 * cc[2]) + cc[0] * (t0 * cb[1] - t1 * cb[2]) +
+                2 * (cb[1] * cc[2] - cb[2] * cc[1]) * (ca[0] + cb[0] * xs + cc[0] * ys);
+    }
+    {  /* _curl_nf1_2d on (0, 1, 2) */
+      const double t0 = ca[2] + cb[2] * xs + cc[2] * ys, t1 = ca[0] + cb[0] * xs + cc[0] * ys;
+      C[7][q] = -cb[1] * (t0 * cc[0] - t1 * cc[2]) + cc[1] * (t0 * cb[0] - t1 * cb[2]) +
+                2 * (cb[0] * cc[2] - cb[2] * cc[0]) * (ca[1] + cb[1] * xs + cc[1] * ys);
+    }
+  }
+  const cplx cf = cf_re + cf_im * I;
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) {
+      double s = 0.0;
+      for (int q = 0; q < 6; ++q) s += C[i][q] * C[j][q] * ABC2_DPTS[0][q];
+      out[8 * i + j] = cf * s * A;
+    }
+}
+
+/* _matrix_builder of robin_abc_order2.py: Mat[itri*64 .. +64] += B(itri) */
+int oracle_abc2_entries(const double *nodes, int64_t nN, const int64_t *tris, int64_t F, const int64_t *btris,
+                        int64_t nb, double cf_re, double cf_im, cplx *Mat) {
+  for (int64_t i = 0; i < nb; ++i) {
+    const int64_t t = btris[i];
+    if (t < 0 || t >= F) return -1;
+    for (int v = 0; v < 3; ++v)
+      if (tris[v * F + t] < 0 || tris[v * F + t] >= nN) return -1;
+  }
+  for (int64_t i = 0; i < nb; ++i) {
+    const int64_t t = btris[i];
+    double X[3][3];
+    for (int d = 0; d < 3; ++d)
+      for (int v = 0; v < 3; ++v) X[d][v] = nodes[d * nN + tris[v * F + t]];
+    cplx B[64];
+    oracle_abc2_block(X, cf_re, cf_im, B);
+    for (int k = 0; k < 64; ++k) Mat[t * 64 + k] += B[k];
   }
   return 0;
 }
