@@ -24,7 +24,7 @@ EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_material_classify", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
-    "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_robin_apply", "emg_robin_force",
+    "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_abc2_build", "emg_robin_apply", "emg_robin_force",
     "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values", "emg_ned2_interp",
     "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol", "emg_coo_build", "emg_coo_finish", "emg_coo_gather",
     "emg_leg2_element",
@@ -122,6 +122,8 @@ def lib():
     L.emg_plan_set_record_width.argtypes = [ctypes.POINTER(Plan), ctypes.c_int]
     L.emg_plan_order.argtypes = [ctypes.POINTER(Plan), _P, _P, _I64, _P, _P, _P, _P]
     L.emg_robin_init.argtypes = [_I64, ctypes.POINTER(Robin)]
+    L.emg_abc2_build.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P,
+                                 _P]
     L.emg_robin_build.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P,
                                   _P]
     L.emg_robin_apply.argtypes = [ctypes.POINTER(Robin), _P, _P, _D, _D, _P, _I64, _P]
@@ -146,7 +148,7 @@ def lib():
                                        ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
     for name in ("emg_device_check", "emg_material_classify", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
-                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build",
+                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_abc2_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
                  "emg_select_values", "emg_ned2_interp", "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol",
                  "emg_coo_build", "emg_coo_finish", "emg_coo_gather", "emg_leg2_element"):

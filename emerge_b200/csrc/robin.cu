@@ -22,6 +22,15 @@ __constant__ double kTL[3][6] = {
     {0.09157621350977004, 0.09157621350977008, 0.81684757298045807, 0.44594849091596500, 0.44594849091596500,
      0.10810301816807000}};
 
+// the second-order ABC correction's own copy of the rule, 14 digits
+// (robin_abc_order2.py:89-98)
+__constant__ double kAW[6] = {0.10995174365532, 0.10995174365532, 0.10995174365532,
+                              0.22338158967801, 0.22338158967801, 0.22338158967801};
+__constant__ double kAL[3][6] = {
+    {0.81684757298046, 0.09157621350977, 0.09157621350977, 0.10810301816807, 0.44594849091597, 0.44594849091597},
+    {0.09157621350977, 0.81684757298046, 0.09157621350977, 0.44594849091597, 0.10810301816807, 0.44594849091597},
+    {0.09157621350977, 0.09157621350977, 0.81684757298046, 0.44594849091597, 0.44594849091597, 0.10810301816807}};
+
 // position of row `row` in column `col` of the CSC pattern, or -1
 __device__ __forceinline__ int64_t find_in_column(const int32_t *indptr, const int32_t *indices, int64_t col,
                                                   int32_t row) {
@@ -43,7 +52,9 @@ struct TriFrame {
   double xh[3], yh[3], tx[3], ty[3], ca[3], cb[3], cc[3];
 };
 
-__device__ double tri_frame(const double *nodes, int64_t nN, const int32_t v[3], TriFrame &T) {
+// abc2: the coefficients as robin_abc_order2.py's tri_coefficients forms them
+// (:100-122: its own signed-area expression, sign and |area| applied apart)
+__device__ double tri_frame(const double *nodes, int64_t nN, const int32_t v[3], TriFrame &T, bool abc2 = false) {
   double X[3][3];
   for (int d = 0; d < 3; ++d)
     for (int k = 0; k < 3; ++k) X[d][k] = nodes[d * nN + v[k]];
@@ -80,12 +91,47 @@ __device__ double tri_frame(const double *nodes, int64_t nN, const int32_t v[3],
   const double a0 = tx[1] * ty[2] - ty[1] * tx[2], a1 = tx[2] * ty[0] - ty[2] * tx[0], a2 = tx[0] * ty[1] - ty[0] * tx[1];
   const double b0 = ty[1] - ty[2], b1 = ty[2] - ty[0], b2 = ty[0] - ty[1];
   const double c0 = tx[2] - tx[1], c1 = tx[0] - tx[2], c2 = tx[1] - tx[0];
+  if (abc2) {
+    const double sA = 0.5 * ((tx[0] - tx[2]) * (ty[1] - ty[0]) - (tx[0] - tx[1]) * (ty[2] - ty[0]));
+    const double sg = sA > 0.0 ? 1.0 : (sA < 0.0 ? -1.0 : 0.0), A2 = 2 * fabs(sA);
+    T.ca[0] = a0 * sg / A2, T.ca[1] = a1 * sg / A2, T.ca[2] = a2 * sg / A2;
+    T.cb[0] = b0 * sg / A2, T.cb[1] = b1 * sg / A2, T.cb[2] = b2 * sg / A2;
+    T.cc[0] = c0 * sg / A2, T.cc[1] = c1 * sg / A2, T.cc[2] = c2 * sg / A2;
+    return fabs(sA);
+  }
   const double sA = 0.5 * (b0 * c1 - b1 * c0);
   const double s2 = 2 * sA;
   T.ca[0] = a0 / s2, T.ca[1] = a1 / s2, T.ca[2] = a2 / s2;
   T.cb[0] = b0 / s2, T.cb[1] = b1 / s2, T.cb[2] = b2 / s2;
   T.cc[0] = c0 / s2, T.cc[1] = c1 / s2, T.cc[2] = c2 / s2;
   return fabs(sA);
+}
+
+// the scalar 2-D curls of the 8 functions at point q of the ABC rule
+// (_curl_ne0_2d, _curl_ne2_2d, _curl_nf0_2d, _curl_nf1_2d, ccbf.py:168-410)
+__device__ __forceinline__ void tri_curls(const TriFrame &T, int q, double C[8]) {
+  const double xs = T.tx[0] * kAL[0][q] + T.tx[1] * kAL[1][q] + T.tx[2] * kAL[2][q];
+  const double ys = T.ty[0] * kAL[0][q] + T.ty[1] * kAL[1][q] + T.ty[2] * kAL[2][q];
+  const int EI[3] = {0, 1, 0}, EJ[3] = {1, 2, 2};
+  const double *a = T.ca, *b = T.cb, *c = T.cc;
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const int i = EI[e], j = EJ[e];
+    C[e] = 2 * b[i] * c[j] - 2 * b[j] * c[i];
+    const double t0 = b[j] * xs, t1 = c[j] * ys, t2 = t0 + t1 + a[j], t3 = a[i] + b[i] * xs + c[i] * ys;
+    C[3 + e] = -(b[i] - b[j]) * (t2 * c[i] - t3 * c[j]) + (c[i] - c[j]) * (t2 * b[i] - t3 * b[j]) +
+               2 * (b[i] * c[j] - b[j] * c[i]) * (-t0 - t1 + t3 - a[j]);
+  }
+  {
+    const double t0 = a[2] + b[2] * xs + c[2] * ys, t1 = a[1] + b[1] * xs + c[1] * ys;
+    C[6] = -b[0] * (t0 * c[1] - t1 * c[2]) + c[0] * (t0 * b[1] - t1 * b[2]) +
+           2 * (b[1] * c[2] - b[2] * c[1]) * (a[0] + b[0] * xs + c[0] * ys);
+  }
+  {
+    const double t0 = a[2] + b[2] * xs + c[2] * ys, t1 = a[0] + b[0] * xs + c[0] * ys;
+    C[7] = -b[1] * (t0 * c[0] - t1 * c[2]) + c[1] * (t0 * b[0] - t1 * b[2]) +
+           2 * (b[0] * c[2] - b[2] * c[0]) * (a[1] + b[1] * xs + c[1] * ys);
+  }
 }
 
 // the 8 Volakis functions (ne0, ne2 on (0,1), (1,2), (0,2); nf0, nf1) at point q
@@ -138,6 +184,12 @@ __device__ __forceinline__ bool tri_load(const int32_t *tris, const int32_t *tri
 // Volakis functions ne0, ne2 on the vertex pairs (0,1), (1,2), (0,2) and
 // nf0, nf1 on (0,1,2) at the 6 points, B[a][b] = A * sum_q w_q f_a . f_b
 // (computed for a <= b and mirrored), and each slot's position in A.
+// ABC2: the second-order ABC correction instead (_abc_order_2_terms,
+// robin_abc_order2.py:143-217), B[a][b] = A * sum_q w_q c_a c_b with c the
+// scalar 2-D curls; the reference's divergence matrix is identically zero
+// (it writes the first function's divergence into a buffer the inner loop
+// overwrites), so the block is the curl term alone.
+template <bool ABC2>
 __global__ void __launch_bounds__(128)
     k_robin_build(const double *nodes, int64_t nN, const int32_t *tris, const int32_t *tri_to_edge, int64_t F,
                   int64_t E, const int32_t *btris, int64_t nb, const int32_t *indptr, const int32_t *indices,
@@ -157,20 +209,31 @@ __global__ void __launch_bounds__(128)
     return;
   }
   TriFrame T;
-  const double area = tri_frame(nodes, nN, v, T);
+  const double area = tri_frame(nodes, nN, v, T, ABC2);
   if (!(area > 0.0) || !isfinite(area)) flag(st, EMG_ST_DEGENERATE, i);
   double B[36];
   for (int k = 0; k < 36; ++k) B[k] = 0.0;
 #pragma unroll 1
   for (int q = 0; q < 6; ++q) {
-    double f[8][2];
-    tri_functions(T, q, f);
-    const double w = kTW[q];
-    int k = 0;
+    if constexpr (ABC2) {
+      double C[8];
+      tri_curls(T, q, C);
+      const double w = kAW[q];
+      int k = 0;
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+      for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int b = a; b < 8; ++b, ++k) B[k] += (f[a][0] * f[b][0] + f[a][1] * f[b][1]) * w;
+        for (int b = a; b < 8; ++b, ++k) B[k] += C[a] * C[b] * w;
+    } else {
+      double f[8][2];
+      tri_functions(T, q, f);
+      const double w = kTW[q];
+      int k = 0;
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = a; b < 8; ++b, ++k) B[k] += (f[a][0] * f[b][0] + f[a][1] * f[b][1]) * w;
+    }
   }
   int64_t dof[8];
   tri_dofs(e, t, E, F, dof);
@@ -297,10 +360,13 @@ int emg_robin_init(int64_t n_btris, emg_robin *r) {
   return EMG_OK;
 }
 
-int emg_robin_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
-                    const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
-                    const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
-                    int64_t *d_status, emg_stream_t stream) {
+}  // extern "C"
+
+namespace {
+int robin_build(bool abc2, const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
+                int64_t *d_status, emg_stream_t stream) {
   if (!r) return fail(EMG_EINVAL, "null robin descriptor");
   if (r->n_btris == 0) return EMG_OK;
   if (!d_nodes || !d_tris || !d_tri_to_edge || !d_btris || !d_indptr || !d_indices || !d_keys || !d_values)
@@ -308,8 +374,15 @@ int emg_robin_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, 
   if (n_nodes <= 0 || n_tris <= 0 || n_edges <= 0 || N != 2 * n_edges + 2 * n_tris)
     return fail(EMG_EINVAL, "bad sizes (N must be 2 E + 2 F)");
   cudaStream_t s = S(stream);
-  k_robin_build<<<grid_for(r->n_btris, 128), 128, 0, s>>>(d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges,
-                                                          d_btris, r->n_btris, d_indptr, d_indices, N, d_keys, static_cast<double2 *>(d_values), d_status);
+  auto *vals = static_cast<double2 *>(d_values);
+  if (abc2)
+    k_robin_build<true><<<grid_for(r->n_btris, 128), 128, 0, s>>>(
+        d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, r->n_btris, d_indptr, d_indices, N, d_keys,
+        vals, d_status);
+  else
+    k_robin_build<false><<<grid_for(r->n_btris, 128), 128, 0, s>>>(
+        d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, r->n_btris, d_indptr, d_indices, N, d_keys,
+        vals, d_status);
   int rc = launch_check("k_robin_build");
   if (rc) return rc;
   if (r->n_keys > r->n_slots) {
@@ -317,6 +390,25 @@ int emg_robin_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, 
     if ((rc = launch_check("k_pad_keys"))) return rc;
   }
   return sort_u64(d_keys, r->n_keys, s);
+}
+}  // namespace
+
+extern "C" {
+
+int emg_robin_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                    const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                    const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
+                    int64_t *d_status, emg_stream_t stream) {
+  return robin_build(false, r, d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, d_indptr, d_indices,
+                     N, d_keys, d_values, d_status, stream);
+}
+
+int emg_abc2_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                   const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                   const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
+                   int64_t *d_status, emg_stream_t stream) {
+  return robin_build(true, r, d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, d_indptr, d_indices,
+                     N, d_keys, d_values, d_status, stream);
 }
 
 int emg_robin_apply(const emg_robin *r, const uint64_t *d_keys, const void *d_values, double gamma_re,

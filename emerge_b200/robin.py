@@ -18,6 +18,15 @@ is linear in gamma, robinbc.py:316-378) and the position in A of each of its
 64 DoF pairs; every assembly then adds gamma times the blocks into A's values
 on the device, summing each position in a fixed order. Every DoF pair of a
 triangle shares a tet with it, so A's pattern does not change.
+
+``RobinTerm(..., kind="abc2")`` is the second-order absorbing boundary
+correction on the same triangles and positions (abc_order_2_matrix,
+robin_abc_order2.py:143-281): the block A sum_q w_q c_a c_b of the scalar
+2-D curls, scaled by the coefficient the assembler passes
+(assembler.py:626-632)::
+
+    R2 = RobinTerm(field, abc_tri_ids, cscmap, kind="abc2")
+    A = cscmap.to_csc(Evec - Bvec * k0**2 + R * gamma + R2 * c2)
 """
 from __future__ import annotations
 
@@ -28,7 +37,7 @@ from scipy.sparse import csc_matrix
 from . import _lib as L
 from .assembly import GpuCSCMapping, LinComb, _to_dev
 
-__all__ = ["RobinTerm", "assemble_robin_bc"]
+__all__ = ["RobinTerm", "assemble_robin_bc", "abc_order_2_matrix"]
 
 # barycentric rows L1..L3 of the 6-point triangle rule (robinbc.py:189-196)
 _TRI_L = np.array([
@@ -48,7 +57,10 @@ class RobinTerm:
 
     _is_robin_term = True
 
-    def __init__(self, field, tri_ids, cscmap: GpuCSCMapping):
+    def __init__(self, field, tri_ids, cscmap: GpuCSCMapping, kind: str = "robin"):
+        if kind not in ("robin", "abc2"):
+            raise ValueError("kind must be 'robin' (the Robin / port term) or 'abc2' (second-order ABC correction)")
+        self.kind = kind
         m = field.mesh
         ids = np.asarray(tri_ids, dtype=np.int64).ravel()
         if ids.size and (ids.min() < 0 or ids.max() >= m.n_tris):
@@ -70,7 +82,8 @@ class RobinTerm:
             self._t2e = _to_dev(m.tri_to_edge, torch.int32, dev)
             self._btris = _to_dev(ids, torch.int32, dev)
             self._status = torch.zeros(2, dtype=torch.int64, device=dev)
-            L.check(L.lib().emg_robin_build(L.ctypes.byref(r), L.ptr(self._nodes), m.n_nodes, L.ptr(self._tris),
+            build = L.lib().emg_abc2_build if kind == "abc2" else L.lib().emg_robin_build
+            L.check(build(L.ctypes.byref(r), L.ptr(self._nodes), m.n_nodes, L.ptr(self._tris),
                                             L.ptr(self._t2e), m.n_tris, m.n_edges, L.ptr(self._btris),
                                             L.ptr(cscmap.d_indptr), L.ptr(cscmap.d_indices), cscmap.N,
                                             L.ptr(self.d_keys), L.ptr(self.d_vals), L.ptr(self._status),
@@ -98,6 +111,8 @@ class RobinTerm:
         """Port forcing vector (assemble_robin_bc_bvec, robinbc.py:405-433):
         b (complex128 [N], device) += the triangles' entries for the incident
         field U (complex [3, 6, n_btris] at ``quadrature_points``)."""
+        if self.kind != "robin":
+            raise ValueError("only the Robin / port term has a forcing vector")
         dev = self.cmap.device
         if b is None:
             b = torch.zeros(self.cmap.N, dtype=torch.complex128, device=dev)
@@ -167,6 +182,14 @@ class RobinTerm:
         """The term alone as a csc_matrix on A's pattern (explicit zeros off the
         boundary; the reference's generate_csc stores only the nonzeros)."""
         return self.cmap.to_csc(self * gamma)
+
+
+def abc_order_2_matrix(field, tri_ids, coeff: complex, cscmap: GpuCSCMapping) -> LinComb:
+    """``coeff`` times the second-order absorbing boundary correction of
+    ``tri_ids`` as a lazy combination (the reference's abc_order_2_matrix,
+    robin_abc_order2.py:259-281, added into its tri matrix and generate_csc'd,
+    assembler.py:626-640), to be added to the element-value combination."""
+    return RobinTerm(field, tri_ids, cscmap, kind="abc2") * coeff
 
 
 def assemble_robin_bc(field, tri_ids, gamma: complex, cscmap: GpuCSCMapping) -> LinComb:

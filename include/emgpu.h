@@ -301,6 +301,18 @@ int emg_robin_build(const emg_robin *robin, const double *d_nodes, int64_t n_nod
                     const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
                     int64_t *d_status, emg_stream_t stream);
 
+/* The second-order absorbing boundary correction in place of the Robin
+ * block, same descriptor, buffers, keys and emg_robin_apply: per triangle
+ * B[a][b] = A sum_q w_q c_a c_b with c the scalar 2-D curls of the 8
+ * functions (abc_order_2_matrix / _abc_order_2_terms,
+ * physics/microwave/assembly/robin_abc_order2.py:143-281, with its own
+ * 14-digit copy of the 6-point rule); apply it with the coefficient the
+ * assembler passes (assembler.py:626-632: c2 = bc.get_abccorr(k0)). */
+int emg_abc2_build(const emg_robin *robin, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                   const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                   const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
+                   int64_t *d_status, emg_stream_t stream);
+
 /* d_A[p] += gamma * (sum of the triangle slots at position p) for the nnz
  * values of A (complex128); stream-ordered, deterministic. */
 int emg_robin_apply(const emg_robin *robin, const uint64_t *d_keys, const void *d_values, double gamma_re,

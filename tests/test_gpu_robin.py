@@ -169,3 +169,53 @@ def test_driven_guide_solution_matches_oracle_system():
     xref = splu(Aref).solve(bref)
     assert np.linalg.norm(x - xref) <= 1e-9 * np.linalg.norm(xref)
     assert np.linalg.norm(Aref @ x - bref) <= 1e-9 * np.linalg.norm(bref)
+
+
+def test_abc2_term_matches_reference_golden():
+    """The second-order ABC correction (kind="abc2") over three faces of the
+    12x6x30 box against the reference's abc_order_2_matrix output; the
+    pattern is A's."""
+    g = load_npz("abc2.npz")
+    wl = W.wr90_air()
+    f = wl.field
+    ids = g["abc_ids"]
+    cf = complex(g["abc_cf"])
+    Mat = np.zeros(f.mesh.n_tris * 64, np.complex128)
+    Mat.reshape(-1, 64)[ids] = g["abc_B"]
+    ref = O.generate_csc(f, Mat)
+    _, _, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    R2 = RobinTerm(f, ids, cmap, kind="abc2")
+    mine = R2.to_csc(cf)
+    assert np.array_equal(mine.indptr, cmap.indptr) and np.array_equal(mine.indices, cmap.indices)
+    fro, mx = _sparse_rel(mine, ref)
+    assert fro <= TOL and mx <= TOL, (fro, mx)
+    with pytest.raises(ValueError):
+        R2.force(np.zeros((3, 6, ids.size), np.complex128))
+    with pytest.raises(ValueError):
+        RobinTerm(f, ids, cmap, kind="abc3")
+
+
+def test_system_with_ports_and_abc2_matches_oracle():
+    """A = K - k0^2 M + gamma R_ports + c2 R_abc2 through the drop-in
+    combination against the oracle's pieces, FP64, on a lossy box."""
+    from scipy.sparse import csc_matrix
+
+    from emerge_b200.mesh import plane_tris
+    from emerge_b200.robin import abc_order_2_matrix
+
+    wl = W.wr90_dielectric(n=(10, 6, 16), seed=7)
+    f = wl.field
+    m = f.mesh
+    ports = W.port_tris(wl)
+    sides = np.concatenate([plane_tris(m, 0, float(m.nodes[0].min())), plane_tris(m, 1, float(m.nodes[1].max()))])
+    k0, gamma, c2 = wl.k0, W.rect_port_gamma(wl.freq), complex(0.02, -0.3)
+    E, B, cmap = tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    A = cmap.to_csc(E - B * k0 ** 2 + RobinTerm(f, ports, cmap) * gamma + abc_order_2_matrix(f, sides, c2, cmap))
+    dE, dB, oc = O.tet_mass_stiffness_matrices(f, wl.er, wl.ur, np.zeros(0, np.int64))
+    K = csc_matrix((oc.values_lincomb(dE, dB, 1.0, -k0 ** 2), oc.indices, oc.indptr), shape=A.shape)
+    ref = (K + O.generate_csc(f, O.robin_entries(f, ports, gamma)) + O.generate_csc(f, O.abc2_entries(f, sides, c2)))
+    ref = ref.tocsc()
+    ref.sort_indices()
+    assert np.array_equal(ref.indptr, A.indptr) and np.array_equal(ref.indices, A.indices)
+    fro, mx = rel_err(A.data, ref.data)
+    assert fro <= 1e-12 and mx <= 1e-12, (fro, mx)
