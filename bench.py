@@ -323,6 +323,23 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         cmap._ws = None  # element workspace of this form
     cmap = cmap8
+    # the mixed form's error against FP64 (which matches the oracle to 1e-12)
+    # for K, M and A, relative Frobenius and max entry, on the device
+    errors = None
+    if "fp64" in results and "mixed" in results:
+        def rel(a, b):
+            d = a - b
+            return {"fro": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(b)),
+                    "max": float(d.abs().max() / b.abs().max())}
+
+        errors = {}
+        for key, ka, kb in (("K", 1.0 + 0j, 0j), ("M", 0j, 1.0 + 0j), ("A", alpha, beta)):
+            v64 = cmap.assemble_device(_Job(dmesh, dmat, L.EMG_FP64), ka, kb).clone()
+            v32 = cmap.assemble_device(_Job(dmesh, dmat, L.EMG_MIXED), ka, kb)
+            errors[key] = rel(v32[: cmap.nnz], v64[: cmap.nnz])
+            del v64, v32
+        cmap._ws = None
+        dmesh.check_status()
     # e2e through the public API (host numpy in, host scipy out), mixed form
     e2e = None
     if args.e2e_steps > 0:
@@ -404,7 +421,7 @@ def run_ours(args, rank, world, local_rank):
                                "k_element_ms": fp["k_element_ms"], "k_gather_ms": fp["k_gather_ms"],
                                "gather_record_bytes": fp["record_bytes"], "roofline": roof(fp, "fp64")},
                 "mixed": {"k_element_ms": mx["k_element_ms"], "k_gather_ms": mx["k_gather_ms"]},
-                "mixed_over_plain": fp["ms"] / mx["ms"],
+                "mixed_over_plain": fp["ms"] / mx["ms"], "mixed_vs_fp64_errors": errors,
                 "roofline": roof(mx, primary), "clocks": mx["clocks"], "e2e": e2e, "gpu_launches": 2 * args.steps}
     return line, wl
 

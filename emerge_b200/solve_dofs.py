@@ -25,7 +25,20 @@ from scipy.sparse import csc_matrix
 from . import _lib as L
 from .assembly import GpuCSCMapping, _to_dev
 
-__all__ = ["SolveSubmatrix"]
+__all__ = ["SolveSubmatrix", "superlu_like_reference"]
+
+
+def superlu_like_reference(A: csc_matrix, b: np.ndarray) -> np.ndarray:
+    """Solve A x = b on the host with scipy's SuperLU under the reference's
+    SolverSuperLU settings without scikit-sparse (solver.py:869-975):
+    MMD_AT_PLUS_A column ordering, relax 0, diagonal pivot threshold 0.001,
+    SymmetricMode, no equilibration, single iterative refinement -- for
+    comparing a GPU-assembled system with the reference's own solve."""
+    from scipy.sparse.linalg import splu
+
+    lu = splu(csc_matrix(A), permc_spec="MMD_AT_PLUS_A", relax=0, diag_pivot_thresh=0.001,
+              options=dict(SymmetricMode=True, Equil=False, IterRefine="SINGLE"))
+    return lu.solve(np.asarray(b))
 
 
 class SolveSubmatrix:
