@@ -544,6 +544,7 @@ def run_pml(args, rank, world, local_rank):
     times = {}
     sampler = ClockSampler(local_rank)
     with sampler:
+        sampler.preroll(lambda: cmap.assemble_device(_Job(dm, dmat, L.EMG_MIXED), alpha, beta, out))
         for name, prec in (("fp64", L.EMG_FP64), ("mixed", L.EMG_MIXED)):
             job = _Job(dm, dmat, prec)
             times[name] = time_steps(lambda: cmap.assemble_device(job, alpha, beta, out), args.steps, args.warmup,
