@@ -807,6 +807,45 @@ def run_shard(args, rank, world, local_rank):
             "clocks": sampler.summary(), "gpu_launches": 2 * args.steps}
 
 
+class CpuServingBaseline:
+    """The same job list through the CPU port of the reference, in arrival
+    order and one job at a time: per job the element build and the pattern,
+    then to_csc(E - k0^2 B) per frequency, all host threads; stops after
+    about budget_s of work and reports the tet-frequencies completed per
+    second."""
+
+    def __init__(self, jobs, budget_s: float = 20.0):
+        self.jobs, self.budget = jobs, budget_s
+        self.cores = os.cpu_count() or 1
+
+    def measure(self):
+        from oracle import oracle as O
+
+        t0 = time.perf_counter()
+        tf = n_jobs = 0
+        for j in self.jobs:
+            f = j.field
+            m = f.mesh
+            dE, dB, rows, cols = O.matrix_builder(m.nodes, m.tets, m.tris, m.edges, f.get_tet_to_field(),
+                                                  m.tet_to_edge, m.tet_to_tri, j.ur, j.er,
+                                                  np.arange(f.ntets, dtype=np.int64), nthreads=self.cores)
+            pat = O.CSCPattern.from_rowcol(rows, cols, f.n_field, self.cores)
+            del rows, cols
+            for fr in j.freqs:
+                if time.perf_counter() - t0 > self.budget:
+                    break
+                k0 = 2 * np.pi * fr / 299792458.0
+                pat.values_lincomb(dE, dB, 1.0, -k0 ** 2, self.cores)
+                tf += f.ntets
+            n_jobs += 1
+            if time.perf_counter() - t0 > self.budget:
+                break
+        dt = time.perf_counter() - t0
+        return {"value": tf / dt, "unit": "tet-freqs/s", "cores": self.cores, "kind": "port",
+                "sample": f"the stream's first {n_jobs} jobs in arrival order, one at a time: element build, "
+                          f"pattern and per-frequency scatter ({tf} tet-frequencies in {dt:.1f} s)"}
+
+
 def run_serving(args, rank, world, local_rank):
     """Serving stream on this rank's GPU (replicas under torchrun: each rank
     serves its own seeded stream). Throughput in tet-frequencies/s."""
@@ -842,6 +881,8 @@ def run_serving(args, rank, world, local_rank):
                        "alloc_conf": os.environ.get("PYTORCH_CUDA_ALLOC_CONF", ""),
                        "parallelism": f"replicas x{world}"},
             "serving": r}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = CpuServingBaseline(jobs).measure()
     return line if rank == 0 else None
 
 
