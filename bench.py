@@ -82,6 +82,7 @@ class ClockSampler:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
+        self.window = "the timed region with its warm-up"
         # nvidia-smi numbers GPUs physically; map a visible-device index
         # through CUDA_VISIBLE_DEVICES when that restricts the visible set
         vis = [x.strip() for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
@@ -112,6 +113,7 @@ class ClockSampler:
 
         if self.proc is None:
             return
+        self.window = "untimed pre-roll steps, warm-up and timed steps of the same workload"
         n0, t0 = len(self.lines), time.perf_counter()
         while len(self.lines) - n0 < min_samples and time.perf_counter() - t0 < max_s:
             step()
@@ -143,7 +145,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
-                "window": "untimed pre-roll steps, warm-up and timed steps of the same workload"}
+                "window": self.window}
 
 
 # ---------------------------------------------------------------- CPU baseline (oracle port)
@@ -880,7 +882,7 @@ def run_serving(args, rank, world, local_rank):
                        "batch_nnz_cap": int(args.serving_batch_nnz),
                        "alloc_conf": os.environ.get("PYTORCH_CUDA_ALLOC_CONF", ""),
                        "parallelism": f"replicas x{world}"},
-            "serving": r}
+            "serving": r, "clocks": r["clocks"]}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = CpuServingBaseline(jobs).measure()
     return line if rank == 0 else None
