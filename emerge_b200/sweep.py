@@ -22,6 +22,7 @@ from . import _lib as L
 from .assembly import ElemValues, GpuCSCMapping
 
 C0 = 299792458.0
+EPS0 = 8.854187818814e-12  # const.py:23 of the reference
 
 
 class FrequencySweep:
@@ -42,6 +43,39 @@ class FrequencySweep:
         for r in self.robin:
             if r.cmap is not cscmap:
                 raise ValueError("a boundary term was built on another mapping")
+
+    @classmethod
+    def with_conductivity(cls, field, er: np.ndarray, tand: np.ndarray, cond: np.ndarray, ur: np.ndarray,
+                          conductor_tets: np.ndarray, cscmap: GpuCSCMapping | None = None, *,
+                          precision: str = "fp64", device=None, robin=None) -> "FrequencySweep":
+        """A sweep over materials with a conductivity, which the reference
+        cannot cache: it forms er(w) = er (1 - j tand) - j cond / (w eps0)
+        and reassembles every frequency (assembler.py:439-456). The mass
+        matrix is linear in er, so with M1 = M[er (1 - j tand)] and
+        P = M[-j cond / eps0], all assembled once here,
+            A(w) = K - k0^2 M1 - (k0^2 / w) P,
+        which ``form(conductive_coefficients(freqs))`` produces per frequency
+        from the three resident matrices (arrays c16[3, 3, n_tets] as the
+        reference's). The excluded conductor tets are the caller's, as in
+        the reference (cond above its PEC limit)."""
+        from .assembly import tet_mass_stiffness_matrices
+
+        er = np.asarray(er, dtype=np.complex128)
+        er1 = er * (1 - 1j * np.asarray(tand, dtype=np.complex128))
+        E, B, cmap = tet_mass_stiffness_matrices(field, er1, ur, conductor_tets, cscmap, precision=precision,
+                                                 device=device)
+        es = -1j * np.asarray(cond, dtype=np.complex128) / EPS0
+        _, Bs, _ = tet_mass_stiffness_matrices(field, es, ur, conductor_tets, cmap, precision=precision, device=device)
+        P = cmap.to_device(Bs).clone()
+        return cls(E, B, cmap, P=P, robin=robin)
+
+    @staticmethod
+    def conductive_coefficients(freqs) -> np.ndarray:
+        """Coefficient rows of K - k0^2 M1 - (k0^2 / w) P (``with_conductivity``)."""
+        f = np.atleast_1d(np.asarray(freqs, dtype=np.float64))
+        w = 2 * np.pi * f
+        k0 = w / C0
+        return FrequencySweep.coefficients(f, gamma=-(k0 ** 2) / w)
 
     @staticmethod
     def coefficients(freqs, gamma=None) -> np.ndarray:
