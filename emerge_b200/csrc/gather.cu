@@ -180,22 +180,40 @@ struct SweepCoef {
   double c[SWEEP_MAX][6];
 };
 
+// Four elements per thread per pass: their loads are independent of the
+// previous pass's stores (restrict), so they are in flight together; the
+// arithmetic per value is unchanged.
 template <bool HASP>
-__global__ void k_form_sweep(const double2 *K, const double2 *M, const double2 *P, int64_t nnz, SweepCoef cf, int nf,
-                             double2 *out, int64_t stride) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x) {
-    double2 k = K[i], m = M[i];
-    double2 p = HASP ? P[i] : make_double2(0.0, 0.0);
+__global__ void __launch_bounds__(256) k_form_sweep(const double2 *__restrict__ K, const double2 *__restrict__ M,
+                                                    const double2 *__restrict__ P, int64_t nnz, SweepCoef cf, int nf,
+                                                    double2 *__restrict__ out, int64_t stride) {
+  constexpr int U = 4;
+  const int64_t T = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < nnz; i0 += U * T) {
+    double2 k[U], m[U], p[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + u * T;
+      const bool in = i < nnz;
+      k[u] = in ? __ldg(K + i) : make_double2(0.0, 0.0);
+      m[u] = in ? __ldg(M + i) : make_double2(0.0, 0.0);
+      p[u] = (HASP && in) ? __ldg(P + i) : make_double2(0.0, 0.0);
+    }
     for (int f = 0; f < nf; ++f) {
       const double *c = cf.c[f];
-      double2 o;
-      o.x = c[0] * k.x - c[1] * k.y + c[2] * m.x - c[3] * m.y;
-      o.y = c[0] * k.y + c[1] * k.x + c[2] * m.y + c[3] * m.x;
-      if (HASP) {
-        o.x += c[4] * p.x - c[5] * p.y;
-        o.y += c[4] * p.y + c[5] * p.x;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t i = i0 + u * T;
+        if (i >= nnz) break;
+        double2 o;
+        o.x = c[0] * k[u].x - c[1] * k[u].y + c[2] * m[u].x - c[3] * m[u].y;
+        o.y = c[0] * k[u].y + c[1] * k[u].x + c[2] * m[u].y + c[3] * m[u].x;
+        if (HASP) {
+          o.x += c[4] * p[u].x - c[5] * p[u].y;
+          o.y += c[4] * p[u].y + c[5] * p[u].x;
+        }
+        out[(int64_t)f * stride + i] = o;
       }
-      out[(int64_t)f * stride + i] = o;
     }
   }
 }
@@ -299,7 +317,7 @@ int launch_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t
     SweepCoef c;
     memcpy(c.c, h_coef + (size_t)f0 * 6, (size_t)n * 6 * sizeof(double));
     double2 *o = static_cast<double2 *>(d_out) + (int64_t)f0 * out_stride;
-    const int g = 148 * 8;
+    const int g = persistent_ctas(8);  // oversubscribed: measured faster than one resident wave
     if (d_P)
       k_form_sweep<true><<<g, 256, 0, s>>>((const double2 *)d_K, (const double2 *)d_M, (const double2 *)d_P, nnz, c,
                                            n, o, out_stride);
