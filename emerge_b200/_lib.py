@@ -74,7 +74,8 @@ class CooMap(ctypes.Structure):
 
 class FormItem(ctypes.Structure):
     _fields_ = [("K", ctypes.c_void_p), ("M", ctypes.c_void_p), ("P", ctypes.c_void_p), ("out", ctypes.c_void_p),
-                ("nnz", ctypes.c_int64), ("coef", ctypes.c_double * 6)]
+                ("nnz", ctypes.c_int64), ("group", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("coef", ctypes.c_double * 6)]
 
 
 FORM_TILE = 32768

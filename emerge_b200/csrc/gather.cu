@@ -232,25 +232,27 @@ __global__ void __launch_bounds__(256) k_form_batch(const emg_form_item *items, 
       const int mid = (lo + hi + 1) >> 1;
       if (tile_start[mid] <= t) lo = mid; else hi = mid - 1;
     }
-    const emg_form_item it = items[lo];
+    const emg_form_item &it = items[lo];
     const int64_t b = (t - tile_start[lo]) * FORM_TILE;
     const int64_t e = min(b + FORM_TILE, it.nnz);
+    const int g = max(1, min(it.group, n - lo));  // the group's items share K, M, P: read them once
     const double2 *K = static_cast<const double2 *>(it.K);
     const double2 *M = static_cast<const double2 *>(it.M);
     const double2 *P = static_cast<const double2 *>(it.P);
-    double2 *out = static_cast<double2 *>(it.out);
-    const double *c = it.coef;
     for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
       const double2 k = K[i], m = M[i];
-      double2 o;
-      o.x = c[0] * k.x - c[1] * k.y + c[2] * m.x - c[3] * m.y;
-      o.y = c[0] * k.y + c[1] * k.x + c[2] * m.y + c[3] * m.x;
-      if (P) {
-        const double2 p = P[i];
-        o.x += c[4] * p.x - c[5] * p.y;
-        o.y += c[4] * p.y + c[5] * p.x;
+      const double2 p = P ? P[i] : make_double2(0.0, 0.0);
+      for (int f = 0; f < g; ++f) {
+        const double *c = items[lo + f].coef;
+        double2 o;
+        o.x = c[0] * k.x - c[1] * k.y + c[2] * m.x - c[3] * m.y;
+        o.y = c[0] * k.y + c[1] * k.x + c[2] * m.y + c[3] * m.x;
+        if (P) {
+          o.x += c[4] * p.x - c[5] * p.y;
+          o.y += c[4] * p.y + c[5] * p.x;
+        }
+        static_cast<double2 *>(items[lo + f].out)[i] = o;
       }
-      out[i] = o;
     }
   }
 }

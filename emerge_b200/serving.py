@@ -350,6 +350,7 @@ class AssemblyServer:
     def _launch(self, batch) -> None:
         tiles = 0
         self._h_tiles[0] = 0
+        lead = 0  # first item of the current run of one job's frequencies (formed together)
         for i, (act, fi, slot) in enumerate(batch):
             k0 = 2 * np.pi * float(act.job.freqs[fi]) / C0
             it = self._items_view[i]
@@ -357,7 +358,13 @@ class AssemblyServer:
             it.out = act.out[slot].data_ptr()
             it.nnz = act.cmap.nnz
             it.coef[:] = (1.0, 0.0, -k0 * k0, 0.0, 0.0, 0.0)
-            tiles += (act.cmap.nnz + L.FORM_TILE - 1) // L.FORM_TILE
+            if i > 0 and batch[i - 1][0] is act:
+                it.group = 0
+                self._items_view[lead].group += 1
+            else:
+                lead = i
+                it.group = 1
+                tiles += (act.cmap.nnz + L.FORM_TILE - 1) // L.FORM_TILE
             self._h_tiles[i + 1] = tiles
         self._h_n[0] = len(batch)
         with torch.cuda.stream(self._batch_stream):

@@ -248,11 +248,16 @@ int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nn
 
 /* One work item of the serving batch: out[i] = a*K[i] + b*M[i] + c*P[i] for
  * i < nnz (complex128; P may be NULL), coef = (a_re, a_im, b_re, b_im, c_re,
- * c_im). 80 bytes. */
+ * c_im). group: on the first of g consecutive items that share K, M, P and
+ * nnz (one job's frequencies), g -- they are formed together, K, M and P read
+ * once -- and 0 on the other g - 1; 1 for an item alone. The tile offsets
+ * give the group's tiles to its first item and none to the others. 88 bytes. */
 typedef struct {
   const void *K, *M, *P;
   void *out;
   int64_t nnz;
+  int32_t group;
+  int32_t reserved;
   double coef[6];
 } emg_form_item;
 
