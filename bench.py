@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--heat", action="store_true",
                     help="Lagrange-2 heat-conduction assembly (stiffness + capacity, COO -> CSC) on a 2.01M-tet box")
     ap.add_argument("--heat-grid", default="100,50,67")
+    ap.add_argument("--shard-emulate", default="",
+                    help="with --shard on one GPU: comma list of shard counts N; each N's shards are assembled one "
+                         "after another and timed (an estimate of N-GPU strong scaling, not a measurement of it)")
     ap.add_argument("--serving", action="store_true",
                     help="serving stream instead: Poisson arrivals of assembly jobs (5k-500k tets, 1-64 frequencies)")
     ap.add_argument("--serving-jobs", type=int, default=50)
@@ -809,6 +812,8 @@ def run_shard(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     wl = make_workload(args.config, grid=args.grid)
     f = wl.field
+    if args.shard_emulate and world == 1:
+        return emulate_shards(args, wl, dev)
     t0 = time.perf_counter()
     sh = shard_of(f.mesh, rank, world, wl.conductor_tets)
     sa = ShardedAssembly(f, wl.er, wl.ur, sh, "mixed", dev)
@@ -833,6 +838,50 @@ def run_shard(args, rank, world, local_rank):
                        "tets_assembled_total": int(tets_done), "halo_overhead": tets_done / f.ntets - 1.0,
                        "setup_s": setup_s},
             "clocks": sampler.summary(), "gpu_launches": 2 * args.steps}
+
+
+def emulate_shards(args, wl, dev):
+    """N-way column shards on one GPU, one after another: each shard's step
+    time (mixed form, its own tets and halo, its own columns). The shards
+    never communicate, so an N-GPU step would take the slowest shard's time;
+    that is reported as an estimate, next to the halo overhead."""
+    import torch
+
+    from emerge_b200.partition import ShardedAssembly, partition
+
+    f = wl.field
+    alpha, beta = 1.0 + 0j, complex(-wl.k0 ** 2)
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    launches = 0
+    for N in [int(x) for x in args.shard_emulate.split(",") if x.strip()]:
+        per, tets, own = [], 0, 0
+        parts = partition(f.mesh, N, wl.conductor_tets)
+        for r in range(N):
+            sh = parts[r]
+            launches += 2 * (args.steps + args.warmup)
+            sa = ShardedAssembly(f, wl.er, wl.ur, sh, "mixed", dev)
+            out = torch.empty(sa.cmap.nnz, dtype=torch.complex128, device=dev)
+            per.append(time_steps(lambda: sa.assemble(alpha, beta, out), args.steps, args.warmup, stream))
+            sa.dmesh.check_status()
+            tets += sh.tetids.size
+            own += sa.own_nnz
+            del sa, out
+            torch.cuda.empty_cache()
+        res[str(N)] = {"shard_ms": per, "step_ms_estimate": max(per), "tets_per_s_estimate": f.ntets / (max(per) * 1e-3),
+                       "halo_overhead": tets / f.ntets - 1.0, "owned_nnz_total": int(own),
+                       "imbalance": max(per) / (sum(per) / N)}
+    one = res.get("1", {}).get("step_ms_estimate")
+    for v in res.values():
+        v["speedup_estimate"] = (one / v["step_ms_estimate"]) if one else None
+    best = max(res.values(), key=lambda v: v["tets_per_s_estimate"])
+    return {"metric": METRIC + " (column shards emulated one after another on one GPU: an estimate)",
+            "value": best["tets_per_s_estimate"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": best["step_ms_estimate"], "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "mixed", "data": "synthetic",
+            "config": {"workload": wl.name, "tets": f.ntets, "hex_grid": list(wl.hex_grid),
+                       "parallelism": "column shards, emulated sequentially"},
+            "emulated_shards": res, "gpu_launches": launches}
 
 
 class CpuServingBaseline:
