@@ -17,7 +17,9 @@ device (latency = arrival -> last A(f) ready).
   copy of its descriptor are captured once in a CUDA graph and replayed per
   batch.
   Each job has a few output slots; an item writes one slot and frees it when
-  the result has been handed over.
+  the result has been handed over. A job's items in one batch form a group:
+  every tile reads that job's K and M once and writes all the group's
+  outputs.
 
 Results are deterministic: every kernel sums in a fixed order and a batch's
 items are independent, so a job's A(f) is bitwise the same alone and in a mix.
