@@ -204,12 +204,22 @@ class GpuCOOMapping:
                                        L.stream_handle(self.device)))
         return out[: self.nnz]
 
-    def to_csc(self, data) -> csc_matrix:
-        """``CSCMapping.to_csc`` (csc_cast.py:55-63)."""
+    def to_csc(self, data, out: np.ndarray | None = None) -> csc_matrix:
+        """``CSCMapping.to_csc`` (csc_cast.py:55-63); ``out``: an optional
+        host array (f8 or c16 [nnz], matching the values) to receive them, as
+        ``GpuCSCMapping.to_csc``."""
         d = self.to_device(data)
-        host = torch.empty(d.shape, dtype=d.dtype, pin_memory=True)
-        host.copy_(d)
-        return csc_matrix((host.numpy(), self.indices, self.indptr), shape=(self.N, self.N))
+        if out is None:
+            host = torch.empty(d.shape, dtype=d.dtype, pin_memory=True)
+            host.copy_(d)
+            vals = host.numpy()
+        else:
+            want = np.complex128 if d.is_complex() else np.float64
+            if out.dtype != want or out.shape != (self.nnz,) or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"out must be a contiguous {np.dtype(want).name} array of {self.nnz} values")
+            torch.from_numpy(out).copy_(d)
+            vals = out
+        return csc_matrix((vals, self.indices, self.indptr), shape=(self.N, self.N))
 
 
 class _HeatMesh:

@@ -172,3 +172,30 @@ def test_repeat_calls_share_device_tets_and_see_moved_nodes():
     E4, B4, c4 = tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64))
     A3, A4 = cmap.to_csc(E3 - B3 * 3.0).data, c4.to_csc(E4 - B4 * 3.0).data
     assert np.array_equal(A3, A4) and not np.array_equal(A3, A1)
+
+
+def test_to_csc_into_a_caller_buffer():
+    """to_csc(..., out=) writes the values into the caller's array (reused
+    across calls) with the same result as the default path; a wrong buffer
+    is refused."""
+    nodes, tets = structured_box(4, 3, 5, jitter=0.1, seed=6)
+    f = Nedelec2Field(TetMesh(nodes, tets))
+    er, ur = _blocky(f.ntets, np.random.default_rng(6))
+    E, B, cmap = tet_mass_stiffness_matrices(f, er, ur, np.zeros(0, np.int64))
+    buf = cmap.host_buffer()
+    for k2 in (1.0, 7.5):
+        A = cmap.to_csc(E - B * k2, out=buf)
+        assert np.shares_memory(A.data, buf)
+        assert np.array_equal(A.data, cmap.to_csc(E - B * k2).data)
+    with pytest.raises(ValueError):
+        cmap.to_csc(E, out=np.zeros(cmap.nnz, np.float64))
+    from emerge_b200.heat import Legrange2, tet_stiffness_matrix
+
+    hf = Legrange2(TetMesh(nodes, tets))
+    cond = np.zeros((3, 3, hf.mesh.n_tets))
+    for d in range(3):
+        cond[d, d] = 2.0
+    K, hmap = tet_stiffness_matrix(hf, cond)
+    hb = np.empty(hmap.nnz, np.float64)
+    H = hmap.to_csc(K, out=hb)
+    assert np.shares_memory(H.data, hb) and np.array_equal(H.data, hmap.to_csc(K).data)
