@@ -109,3 +109,28 @@ def test_full_size_sweep_with_ports():
         d = A[i] - direct
         assert float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(direct)) <= 1e-13
         assert float(d.abs().max() / direct.abs().max()) <= 1e-13
+
+
+def test_full_size_heat_properties():
+    """The 2.01M-tet Lagrange-2 heat box: K 1 = 0 (the basis sums to one), the
+    entries of M sum to sum_q w_q * sum_t rho_cp V_t (the reference's 8-digit
+    weights), the two element forms agree to 1e-9 (they differ by the
+    reference's own rounding, which grows with the mesh's offset/size ratio)."""
+    from emerge_b200.heat import tet_mass_matrix, tet_stiffness_matrix
+
+    wl = W.heat_box()
+    f = wl.field
+    m = f.mesh
+    K, cmap = tet_stiffness_matrix(f, wl.cond)
+    Kx, _ = tet_stiffness_matrix(f, wl.cond, precision="exact")
+    kv, kxv = cmap.to_device(K), cmap.to_device(Kx)
+    assert float((kxv - kv).abs().max() / kv.abs().max()) <= 1e-9
+    ptr = torch.from_numpy(cmap.indptr.astype(np.int64)).to(kv.device)
+    col = torch.repeat_interleave(torch.arange(cmap.N, device=kv.device), ptr[1:] - ptr[:-1])
+    row_sums = torch.zeros(cmap.N, dtype=torch.float64, device=kv.device).index_add_(0, col, kv)  # K^T 1 = K 1
+    assert float(row_sums.abs().max()) <= 1e-9 * float(kv.abs().max())
+    M, _ = tet_mass_matrix(f, wl.rho_cp)
+    X = m.nodes[:, m.tets]
+    V = np.abs(np.einsum("it,it->t", X[:, 1] - X[:, 0], np.cross(X[:, 2] - X[:, 0], X[:, 3] - X[:, 0], axis=0))) / 6
+    expect = (-0.078933 + 4 * 0.04573333 + 6 * 0.14933333) * float((wl.rho_cp * V).sum())
+    assert abs(float(cmap.to_device(M).sum()) - expect) <= 1e-10 * expect
