@@ -143,10 +143,22 @@ class GpuCOOMapping:
 
     @staticmethod
     def from_rowcol(rows, cols, N: int, device=None) -> "GpuCOOMapping":
+        """The mapping of a slot list (int rows, cols in [0, N); numpy arrays
+        or device tensors). Indices are checked before they are narrowed to
+        int32, so none can wrap into range."""
         dev = _device(device)
-        r = rows if isinstance(rows, torch.Tensor) else _to_dev(np.asarray(rows), torch.int32, dev)
-        c = cols if isinstance(cols, torch.Tensor) else _to_dev(np.asarray(cols), torch.int32, dev)
-        return GpuCOOMapping(r.to(dev), c.to(dev), N)
+        out = []
+        for a in (rows, cols):
+            if isinstance(a, torch.Tensor):
+                if a.numel() and (int(a.min()) < 0 or int(a.max()) >= N):
+                    raise L.EmgMeshError(L.EMG_EMESH, "COO index outside [0, N)")
+                out.append(a.to(device=dev, dtype=torch.int32))
+            else:
+                h = np.asarray(a)
+                if h.size and (h.min() < 0 or h.max() >= N):
+                    raise L.EmgMeshError(L.EMG_EMESH, "COO index outside [0, N)")
+                out.append(_to_dev(h, torch.int32, dev))
+        return GpuCOOMapping(out[0], out[1], N)
 
     @staticmethod
     def from_tet_to_field(tet_to_field, N: int, device=None) -> "GpuCOOMapping":

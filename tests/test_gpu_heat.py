@@ -123,6 +123,10 @@ def test_empty_and_out_of_range_slots():
         GpuCOOMapping.from_rowcol(np.array([0, 1]), np.array([0, 5]), 5, device="cuda")
     with pytest.raises(L.EmgMeshError):
         GpuCOOMapping.from_rowcol(np.array([0, -1]), np.array([0, 1]), 5, device="cuda")
+    with pytest.raises(L.EmgMeshError):  # would wrap to 5 in int32
+        GpuCOOMapping.from_rowcol(np.array([0, 2 ** 32 + 1]), np.array([0, 1]), 5, device="cuda")
+    with pytest.raises(L.EmgMeshError):
+        GpuCOOMapping.from_rowcol(torch.tensor([0, 1]), torch.tensor([0, 2 ** 32 + 1]), 5, device="cuda")
 
 
 def test_partitioned_numbering_matches_oracle():
