@@ -101,7 +101,10 @@ class DeviceMesh:
                 and reuse.n_tets == self.n_tets):
             self.tets = reuse.tets
         else:
-            self.tets = _to_dev(mesh.tets, torch.int32, dev, alloc)
+            t = np.asarray(mesh.tets)
+            if t.size and (t.min() < 0 or t.max() >= self.n_nodes):  # before narrowing to int32
+                raise IndexError("tet node index outside [0, n_nodes)")
+            self.tets = _to_dev(t, torch.int32, dev, alloc)
         self.tetids_host = _tet_assy(self.n_tets, conductor_tets)
         self.n_assy = int(self.tetids_host.shape[0]) if self.tetids_host is not None else self.n_tets
         self.tetids = _to_dev(self.tetids_host, torch.int32, dev, alloc) if self.tetids_host is not None else None
