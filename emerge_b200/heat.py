@@ -247,7 +247,10 @@ class _HeatMesh:
         if t2f.shape[1] != self.n_tets:
             raise ValueError("tet_to_field and mesh.tets differ in tet count")
         self.nodes = _to_dev(np.asarray(m.nodes, dtype=np.float64), torch.float64, device)
-        self.tets = _to_dev(np.asarray(m.tets), torch.int32, device)
+        t = np.asarray(m.tets)
+        if t.size and (t.min() < 0 or t.max() >= self.n_nodes):  # before narrowing to int32
+            raise IndexError("tet node index outside [0, n_nodes)")
+        self.tets = _to_dev(t, torch.int32, device)
         self.cmap = GpuCOOMapping.from_tet_to_field(t2f, int(field.n_field), device)
         self.key = (id(m.nodes), id(m.tets), id(field.tet_to_field), int(field.n_field))
 
