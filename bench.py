@@ -242,12 +242,69 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------- GPU arm
-def time_steps(fn, steps, warmup, stream):
+L2_BYTES = 126 * 10 ** 6
+
+
+class L2Guard:
+    """Timing hygiene for a step whose data could stay in the 126 MB L2 from
+    one step to the next: when the bytes a step reads and writes are below 16
+    L2 sizes, a 256 MB buffer is written on the launching stream before every
+    timed step or kernel, outside the timed events. Larger steps are timed
+    back to back (their inputs are larger than L2)."""
+
+    def __init__(self, footprint, dev):
+        import torch
+
+        self.footprint = int(footprint)
+        self.buf = None
+        if self.footprint < 16 * L2_BYTES:
+            self.buf = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=dev)
+        self.n = 0
+
+    @property
+    def active(self):
+        return self.buf is not None
+
+    def flush(self, stream):
+        import torch
+
+        if self.buf is not None:
+            self.n += 1
+            with torch.cuda.stream(stream):
+                self.buf.fill_(self.n & 0xFF)
+
+    def text(self):
+        if self.buf is None:
+            return (f"inputs larger than L2: {self.footprint / 1e9:.2f} GB read or written per step "
+                    f"against 126 MB of L2, steps timed back to back")
+        return (f"L2 flushed before every timed step and kernel (256 MB written outside the timed events); "
+                f"step footprint {self.footprint / 1e6:.0f} MB")
+
+
+def assembly_footprint(cmap, prec):
+    """Bytes one assembly step reads or writes: the element values written
+    and read back, the plan read, A written."""
+    from emerge_b200 import _lib as L
+
+    ws = int(L.lib().emg_assemble_workspace_size(cmap.n_assy, prec))
+    return cmap.d_plan.numel() * cmap.d_plan.element_size() + 2 * ws + 16 * cmap.nnz
+
+
+def time_steps(fn, steps, warmup, stream, l2=None):
     import torch
 
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
+    if l2 is not None and l2.active:
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in evs:
+            l2.flush(stream)
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / steps
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(steps):
@@ -257,9 +314,10 @@ def time_steps(fn, steps, warmup, stream):
     return ev0.elapsed_time(ev1) / steps
 
 
-def kernel_times(cmap, job, prec, alpha, beta, out, reps, stream):
+def kernel_times(cmap, job, prec, alpha, beta, out, reps, stream, l2=None):
     """Average duration of each kernel of the step, CUDA events on the
-    launching stream."""
+    launching stream (L2 flushed before each repetition when the guard
+    asks for it)."""
     import torch
 
     from emerge_b200 import _lib as L
@@ -272,6 +330,8 @@ def kernel_times(cmap, job, prec, alpha, beta, out, reps, stream):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     te, tg = 0.0, 0.0
     for _ in range(reps):
+        if l2 is not None:
+            l2.flush(stream)
         ev[0].record(stream)
         L.check(lib.emg_element_values(L.ptr(m.nodes), m.n_nodes, L.ptr(m.tets), m.n_tets, L.ptr(m.tetids),
                                        m.n_assy, L.ctypes.byref(mat), prec, L.EMG_OUT_LINCOMB, L.EMG_LAYOUT_PACKED,
@@ -333,6 +393,7 @@ def run_ours(args, rank, world, local_rank):
             cmaps[width] = GpuCSCMapping(dmesh, record_bytes=width)
         cmap = cmaps[width]
         cmap.workspace(prec)
+        l2 = L2Guard(assembly_footprint(cmap, prec), dev)
 
         def step():
             cmap.assemble_device(job, alpha, beta, out)
@@ -344,7 +405,7 @@ def run_ours(args, rank, world, local_rank):
         if sampler:
             sampler.__enter__()
             sampler.preroll(step)
-        ms = time_steps(step, args.steps, args.warmup, stream)
+        ms = time_steps(step, args.steps, args.warmup, stream, l2)
         if sampler:
             sampler.__exit__()
         if world > 1:
@@ -352,9 +413,10 @@ def run_ours(args, rank, world, local_rank):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         dmesh.check_status()
-        te, tg = kernel_times(cmap, job, prec, alpha, beta, out, 3, stream)
+        te, tg = kernel_times(cmap, job, prec, alpha, beta, out, 3, stream, l2)
         results[pname] = {"ms": ms, "k_element_ms": te, "k_gather_ms": tg, "record_bytes": width,
-                          "clocks": sampler.summary() if sampler else None}
+                          "clocks": sampler.summary() if sampler else None, "l2": l2.text()}
+        del l2
         torch.cuda.synchronize()
         cmap._ws = None  # element workspace of this form
     cmap = cmap8
@@ -448,7 +510,7 @@ def run_ours(args, rank, world, local_rank):
                 "vs_baseline": None, "dtype": "f64 geometry + f32 contraction (mixed), f64 sum", "data": "synthetic",
                 "config": {"workload": wl.name, "tets": nT, "hex_grid": list(wl.hex_grid), "nnz": nnz,
                            "N": f.n_field, "freq_hz": wl.freq, "form": primary,
-                           "l2": "inputs larger than L2 (packed element values 6.75 GB fp64 / 3.4 GB mixed, A 8.9 GB per step)",
+                           "l2": mx["l2"],
                            "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
                            "alg_bytes_per_step": balg, "floor_bytes_per_step": bfloor,
                            "plan_build_s": plan_s},
@@ -517,17 +579,18 @@ def run_sweep(args, rank, world, local_rank):
             g = gam[i0:i0 + nb]
             sw.form(coef_fn(fb), out[: fb.size], robin_gamma=np.stack([g, g], axis=1))
 
-    sampler = ClockSampler(local_rank)
-    with sampler:
-        ms = time_steps(sweep, args.steps, args.warmup, stream)
-    cmap.dmesh.check_status()
-    ms = max_over_ranks([ms], dev)[0]
-    if rank != 0:
-        return None, None
     nnz, nf = cmap.nnz, freqs.size
     n_launch = -(-nf // nb)
     n_res = 3 if args.sweep_conductive else 2  # resident matrices read per launch
     bytes_sweep = n_launch * 16 * n_res * nnz + nf * 16 * nnz  # K, M (, P) read per batch; A written per frequency
+    l2 = L2Guard(bytes_sweep, dev)
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        ms = time_steps(sweep, args.steps, args.warmup, stream, l2)
+    cmap.dmesh.check_status()
+    ms = max_over_ranks([ms], dev)[0]
+    if rank != 0:
+        return None, None
     hbm = (json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
            if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else None) or 6650.0
     ach = bytes_sweep / (ms * 1e-3) / 1e9
@@ -541,7 +604,7 @@ def run_sweep(args, rank, world, local_rank):
             "config": {"workload": wl.name + ("_conductive_sweep" if args.sweep_conductive else "_sweep"),
                        "tets": f.ntets, "nnz": nnz, "freqs": nf,
                        "band_hz": [8e9, 12e9], "batch": nb, "port_tris": int(sum(r.n_btris for r in ports)),
-                       "K_M_form": "fp64", "setup_s": setup_s,
+                       "K_M_form": "fp64", "setup_s": setup_s, "l2": l2.text(),
                        "step": f"all {nf} frequencies, {n_launch} form launches + {2 * nf} port-term launches"},
             "tet_freqs_per_s": world * f.ntets * nf / (ms * 1e-3),
             "roofline": {"bound": "hbm", "kernel": "k_form_sweep", "achieved": ach, "peak": hbm, "unit": "GB/s",
@@ -572,14 +635,17 @@ def run_pml(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     dmat = DeviceMaterial(wl.er, wl.ur, f.ntets, dev)
     out = torch.empty(cmap.nnz, dtype=torch.complex128, device=dev)
-    times = {}
+    times, l2s = {}, {}
     sampler = ClockSampler(local_rank)
     with sampler:
         sampler.preroll(lambda: cmap.assemble_device(_Job(dm, dmat, L.EMG_MIXED), alpha, beta, out))
         for name, prec in (("fp64", L.EMG_FP64), ("mixed", L.EMG_MIXED)):
             job = _Job(dm, dmat, prec)
+            l2 = L2Guard(assembly_footprint(cmap, prec), dev)
             times[name] = time_steps(lambda: cmap.assemble_device(job, alpha, beta, out), args.steps, args.warmup,
-                                     stream)
+                                     stream, l2)
+            l2s[name] = l2.text()
+            del l2
     dm.check_status()
     times = dict(zip(times, max_over_ranks(list(times.values()), dev)))
 
@@ -617,7 +683,7 @@ def run_pml(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "mixed", "data": "synthetic",
             "config": {"workload": wl.name, "tets": nT, "hex_grid": list(wl.hex_grid), "nnz": nnz,
                        "slivers": int(len(wl.slivers)), "material": "diagonal complex er = ur (PML shell)",
-                       "alg_bytes_per_step": balg},
+                       "alg_bytes_per_step": balg, "l2": l2s["mixed"]},
             "plain_fp64": {"value": world * nT / (times["fp64"] * 1e-3), "ms_per_step": times["fp64"]},
             "mixed_vs_fp64_errors": errors, "clocks": sampler.summary(), "gpu_launches": 4 * args.steps}, wl
 
@@ -664,8 +730,22 @@ def run_heat(args, rank, world, local_rank):
         L.check(lib.emg_coo_gather(L.ctypes.byref(cm.desc), L.ptr(cm.d_perm), L.ptr(cm.d_run), 0, 10, L.ptr(v),
                                    L.ptr(out), sh))
 
+    # both element matrices written and read back, the map read twice, K and M written
+    l2 = L2Guard(4 * 800 * nT + 2 * (4 * cm.d_perm.numel() + 4 * cm.d_run.numel()) + 16 * nnz, dev)
+
     def ktime(fn, reps=5):
         fn()
+        if l2.active:
+            tot = 0.0
+            for _ in range(reps):
+                l2.flush(stream)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                torch.cuda.synchronize()
+                tot += a.elapsed_time(b)
+            return tot / reps
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         for _ in range(reps):
@@ -686,7 +766,7 @@ def run_heat(args, rank, world, local_rank):
         if pname == "exact":
             sampler.__enter__()
             sampler.preroll(step)
-        ms = time_steps(step, args.steps, args.warmup, stream)
+        ms = time_steps(step, args.steps, args.warmup, stream, l2)
         if pname == "exact":
             sampler.__exit__()
         ms = max_over_ranks([ms], dev)[0]
@@ -751,7 +831,7 @@ def run_heat(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": wl.name, "tets": nT, "hex_grid": list(wl.hex_grid), "N": int(f.n_field),
                        "nnz": nnz, "form": "exact", "setup_s": setup_s,
-                       "l2": "inputs larger than L2 (1.6 GB of element values per matrix)",
+                       "l2": l2.text(),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 gpu"},
             "plain_fp64": {"value": world * nT / (fp["ms"] * 1e-3), "ms_per_step": fp["ms"],
                            "k_stiff_ms": fp["k_stiff_ms"], "k_mass_ms": fp["k_mass_ms"],
@@ -822,9 +902,10 @@ def run_shard(args, rank, world, local_rank):
     alpha, beta = 1.0 + 0j, complex(-wl.k0 ** 2)
     out = torch.empty(sa.cmap.nnz, dtype=torch.complex128, device=dev)
     stream = torch.cuda.current_stream(dev)
+    l2 = L2Guard(assembly_footprint(sa.cmap, sa.job.precision), dev)
     sampler = ClockSampler(local_rank)
     with sampler:
-        ms = time_steps(lambda: sa.assemble(alpha, beta, out), args.steps, args.warmup, stream)
+        ms = time_steps(lambda: sa.assemble(alpha, beta, out), args.steps, args.warmup, stream, l2)
     sa.dmesh.check_status()
     ms, setup_s = max_over_ranks([ms, setup_s], dev)
     own, tets_done = sum_over_ranks([sa.own_nnz, sh.tetids.size], dev)
@@ -836,7 +917,7 @@ def run_shard(args, rank, world, local_rank):
             "config": {"workload": wl.name, "tets": f.ntets, "hex_grid": list(wl.hex_grid),
                        "parallelism": f"column shards x{world}", "owned_nnz_total": int(own),
                        "tets_assembled_total": int(tets_done), "halo_overhead": tets_done / f.ntets - 1.0,
-                       "setup_s": setup_s},
+                       "setup_s": setup_s, "l2": l2.text()},
             "clocks": sampler.summary(), "gpu_launches": 2 * args.steps}
 
 
@@ -855,14 +936,17 @@ def emulate_shards(args, wl, dev):
     res = {}
     launches = 0
     for N in [int(x) for x in args.shard_emulate.split(",") if x.strip()]:
-        per, tets, own = [], 0, 0
+        per, tets, own, l2_text = [], 0, 0, []
         parts = partition(f.mesh, N, wl.conductor_tets)
         for r in range(N):
             sh = parts[r]
             launches += 2 * (args.steps + args.warmup)
             sa = ShardedAssembly(f, wl.er, wl.ur, sh, "mixed", dev)
             out = torch.empty(sa.cmap.nnz, dtype=torch.complex128, device=dev)
-            per.append(time_steps(lambda: sa.assemble(alpha, beta, out), args.steps, args.warmup, stream))
+            l2 = L2Guard(assembly_footprint(sa.cmap, sa.job.precision), dev)
+            l2_text.append(l2.text())
+            per.append(time_steps(lambda: sa.assemble(alpha, beta, out), args.steps, args.warmup, stream, l2))
+            del l2
             sa.dmesh.check_status()
             tets += sh.tetids.size
             own += sa.own_nnz
@@ -870,7 +954,7 @@ def emulate_shards(args, wl, dev):
             torch.cuda.empty_cache()
         res[str(N)] = {"shard_ms": per, "step_ms_estimate": max(per), "tets_per_s_estimate": f.ntets / (max(per) * 1e-3),
                        "halo_overhead": tets / f.ntets - 1.0, "owned_nnz_total": int(own),
-                       "imbalance": max(per) / (sum(per) / N)}
+                       "imbalance": max(per) / (sum(per) / N), "l2": l2_text}
     one = res.get("1", {}).get("step_ms_estimate")
     for v in res.values():
         v["speedup_estimate"] = (one / v["step_ms_estimate"]) if one else None
@@ -880,7 +964,8 @@ def emulate_shards(args, wl, dev):
             "warmup": args.warmup, "ms_per_step": best["step_ms_estimate"], "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "mixed", "data": "synthetic",
             "config": {"workload": wl.name, "tets": f.ntets, "hex_grid": list(wl.hex_grid),
-                       "parallelism": "column shards, emulated sequentially"},
+                       "parallelism": "column shards, emulated sequentially",
+                       "l2": "per shard, in emulated_shards[N].l2"},
             "emulated_shards": res, "gpu_launches": launches}
 
 
