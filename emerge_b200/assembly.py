@@ -500,6 +500,5 @@ def tet_mass_stiffness_matrices(field, er: np.ndarray, ur: np.ndarray, conductor
     dmat = DeviceMaterial(er, ur, dmesh.n_tets, dmesh.device)
     job = _Job(dmesh, dmat, _prec(precision))
     if cscmap is None:
-        # compact 4-byte gather records are faster for complex128 element values
-        cscmap = GpuCSCMapping(dmesh, record_bytes=8 if job.precision == L.EMG_MIXED else 4)
+        cscmap = GpuCSCMapping(dmesh, record_bytes=8)
     return ElemValues(job, "K"), ElemValues(job, "M"), cscmap

@@ -3,6 +3,7 @@
 // Replaces CSCMapping.to_csc / scatter_to_csc_c16 (mth/csc_cast.py:55-63,
 // 162-177) and the caller's COO combination Evec - Bvec*k0^2
 // (physics/microwave/assembly/assembler.py:494).
+#include <type_traits>
 #include "common.cuh"
 
 namespace emg {
@@ -129,8 +130,13 @@ __global__ void __launch_bounds__(PG_WARPS * 32)
 // bit, the second slot from kSecondSlot)
 __constant__ SecondSlotTable kSecondSlot = make_second_slot_table();
 
+// Complex128 values (R = double): the list bounds of a lane's next position
+// are loaded while the current one is summed, which takes one dependent load
+// off each position's chain, with the register count held for six CTAs per
+// SM. Complex64 values keep the plain loop (32 registers and eight CTAs per SM
+// with 8-byte records), where the prefetch measured slower.
 template <typename R, bool COMPACT>
-__global__ void __launch_bounds__(PG_WARPS * 32)
+__global__ void __launch_bounds__(PG_WARPS * 32, (std::is_same<R, double>::value || COMPACT) ? 6 : 8)
     k_gather_packed(const int32_t *ent_ptr, const int32_t *order, const void *pidx_v, const uint16_t *posoff,
                     int64_t E, int64_t F, int64_t n_values, const int32_t *indptr, const void *v, double ar,
                     double ai, double2 *A) {
@@ -143,9 +149,25 @@ __global__ void __launch_bounds__(PG_WARPS * 32)
   ChunkMeta m;
   if (!chunk_meta(ent_ptr, order, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
   const int total = 20 * (m.I1 - m.I0);
+  constexpr bool PREFETCH = std::is_same<R, double>::value;
+  int n0 = 0, n1 = 0;
+  if (PREFETCH && lane < m.Lsum) {
+    n0 = posoff[m.hbase + lane];
+    n1 = lane + 1 < m.Lsum ? (int)posoff[m.hbase + lane + 1] : total;
+  }
   for (int p = lane; p < m.Lsum; p += 32) {
-    const int o0 = posoff[m.hbase + p];
-    const int o1 = min(p + 1 < m.Lsum ? (int)posoff[m.hbase + p + 1] : total, total);
+    int o0, o1;
+    if constexpr (PREFETCH) {
+      o0 = n0;
+      o1 = min(n1, total);
+      if (p + 32 < m.Lsum) {
+        n0 = posoff[m.hbase + p + 32];
+        n1 = p + 33 < m.Lsum ? (int)posoff[m.hbase + p + 33] : total;
+      }
+    } else {
+      o0 = posoff[m.hbase + p];
+      o1 = min(p + 1 < m.Lsum ? (int)posoff[m.hbase + p + 1] : total, total);
+    }
     double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
     for (int k = o0; k < o1; ++k) {
       int64_t qx, qy;
