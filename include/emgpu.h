@@ -150,10 +150,11 @@ int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tri
 /* Host-only, between emg_plan_init and emg_plan_build: the width of the
  * packed gather's per-contribution record. 8 bytes (default) store both value
  * indices; 4 bytes store the first and a bit, the second is derived on chip
- * (at most 10,226,078 assembled tets). 4 bytes halve that stream and are
- * faster for complex128 element values (plain FP64 / exact), 8 bytes are
- * faster for complex64 (mixed). Values are identical either way. Updates
- * plan_bytes. No counterpart in the reference. */
+ * (at most 10,226,078 assembled tets). 4 bytes halve that stream and the
+ * plan's largest part, at some gather speed (the on-chip decode lengthens
+ * each position's chain of dependent loads): 8 bytes are the faster width
+ * for every form. Values are identical either way. Updates plan_bytes. No
+ * counterpart in the reference. */
 int emg_plan_set_record_width(emg_plan *plan, int bytes);
 
 /* Builds the entity->tet incidence lists, column lengths and indptr[N+1]
