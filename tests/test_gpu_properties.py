@@ -199,3 +199,49 @@ def test_to_csc_into_a_caller_buffer():
     hb = np.empty(hmap.nnz, np.float64)
     H = hmap.to_csc(K, out=hb)
     assert np.shares_memory(H.data, hb) and np.array_equal(H.data, hmap.to_csc(K).data)
+
+
+def _orient(nodes, tets):
+    """Reorder each tet to a positive determinant (the reference's meshes
+    come that way from gmsh)."""
+    tets = tets.copy()
+    X = nodes[:, tets]
+    det = np.einsum("it,it->t", X[:, 1] - X[:, 0], np.cross(X[:, 2] - X[:, 0], X[:, 3] - X[:, 0], axis=0))
+    flip = det < 0
+    tets[1, flip], tets[2, flip] = tets[2, flip].copy(), tets[1, flip].copy()
+    return tets
+
+
+@pytest.mark.parametrize("n_tets", [1, 2])
+def test_one_and_two_tet_meshes_full_tensors(n_tets):
+    """The smallest meshes: one tet (A is its dense 20x20 block, nnz 400) and
+    two tets sharing a face, with full (non-diagonal) complex er and ur, in
+    both forms against the oracle."""
+    rng = np.random.default_rng(40 + n_tets)
+    base = np.array([[0.0, 1.0, 0.0, 0.0, 0.9], [0.0, 0.0, 1.0, 0.0, 0.8], [0.0, 0.0, 0.0, 1.0, 0.7]]) * 1e-3
+    nodes = base + rng.uniform(-0.1e-3, 0.1e-3, base.shape)
+    tets = np.array([[0, 1], [1, 2], [2, 3], [3, 4]], np.int64)[:, :n_tets]
+    if n_tets == 1:
+        nodes = nodes[:, :4]
+    tets = _orient(nodes, tets)
+    f = Nedelec2Field(TetMesh(nodes, tets))
+    er = rng.uniform(1, 4, (3, 3, n_tets)) + 1j * rng.uniform(-0.2, 0.2, (3, 3, n_tets))
+    ur = rng.uniform(-0.3, 0.3, (3, 3, n_tets)) + 1j * rng.uniform(-0.1, 0.1, (3, 3, n_tets))
+    for d in range(3):
+        ur[d, d] += 2.0
+    none = np.zeros(0, np.int64)
+    m = f.mesh
+    E, B, cmap = tet_mass_stiffness_matrices(f, er, ur, none)
+    dE, dB, ocmap = O.tet_mass_stiffness_matrices(f, er, ur, none)
+    assert cmap.nnz == 4 * m.n_edges + 52 * m.n_tris + 168 * n_tets
+    assert np.array_equal(cmap.indptr, ocmap.indptr) and np.array_equal(cmap.indices, ocmap.indices)
+    if n_tets == 1:
+        assert cmap.nnz == 400 and np.all(np.diff(cmap.indptr) == 20)
+    k2 = (2 * np.pi * 10e9 / 299792458.0) ** 2
+    for precision, tol in (("fp64", 1e-12), ("mixed", 1e-6)):
+        E, B, _ = tet_mass_stiffness_matrices(f, er, ur, none, cmap, precision=precision)
+        for a, (ra, rb) in ((E * 1.0, (1.0, 0.0)), (B * 1.0, (0.0, 1.0)), (E - B * k2, (1.0, -k2))):
+            got = cmap.to_csc(a).data
+            want = ocmap.values_lincomb(dE, dB, ra, rb)
+            fro, mx = rel_err(got, want)
+            assert fro <= tol and mx <= tol, (precision, ra, rb, fro, mx)

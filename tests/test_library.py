@@ -39,3 +39,17 @@ def test_host_only_entry_points():
     assert lib.emg_plan_set_record_width(ctypes.byref(p), 3) == L.EMG_EINVAL
     assert lib.emg_assemble_workspace_size(10, L.EMG_FP64) == 10 * 210 * 16
     assert lib.emg_assemble_workspace_size(10, L.EMG_MIXED) == 10 * 210 * 8
+
+
+def test_size_limits_are_range_errors():
+    """Meshes beyond 32-bit indexing are refused on the host, before any
+    device work: 400 slots per assembled tet must fit int32 (the reference
+    COO slot index), and so must the DoF count 2(E + F)."""
+    lib = L.lib()
+    p = L.Plan()
+    top = (2 ** 31 - 1) // 400
+    assert lib.emg_plan_init(top, top, 100, 100, ctypes.byref(p)) == 0
+    assert lib.emg_plan_init(top + 1, top + 1, 100, 100, ctypes.byref(p)) == L.EMG_ERANGE
+    assert b"too large" in lib.emg_last_error()
+    assert lib.emg_plan_init(10, 10, 2 ** 29, 2 ** 29, ctypes.byref(p)) == L.EMG_ERANGE
+    assert lib.emg_plan_init(10, 11, 100, 100, ctypes.byref(p)) == L.EMG_EINVAL
