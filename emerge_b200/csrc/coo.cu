@@ -92,10 +92,23 @@ __device__ __forceinline__ int64_t value_index(int32_t s) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(256) k_coo_gather_f8(const int32_t *perm, const int32_t *run, int64_t nnz,
-                                                       int64_t S, const double *vals, double *out) {
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t b = run[p], e = min((int64_t)run[p + 1], S);
+__global__ void __launch_bounds__(256, 8) k_coo_gather_f8(const int32_t *perm, const int32_t *run, int64_t nnz,
+                                                          int64_t S, const double *vals, double *out) {
+  // the run bounds of this thread's next entry are loaded while the current
+  // entry is summed (one dependent load off each entry's chain)
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int32_t nb = 0, ne = 0;
+  if (p < nnz) {
+    nb = run[p];
+    ne = run[p + 1];
+  }
+  for (; p < nnz; p += stride) {
+    const int32_t b = nb, e = min((int64_t)ne, S);
+    if (p + stride < nnz) {
+      nb = run[p + stride];
+      ne = run[p + stride + 1];
+    }
     double s = 0.0;
     int32_t i = b;
     for (; i + 4 <= e; i += 4) {  // four loads in flight, summed in slot order
