@@ -355,12 +355,35 @@ HeatRule make_heat_rule() {
 
 // one thread per tet, its 100 values staged per block (value-major, so the
 // staging writes do not conflict) and stored coalesced
-__global__ void __launch_bounds__(kExactTets) k_leg2_exact(const double *nodes, int64_t nN, const int32_t *tets,
-                                                           int64_t nT, const double *coef, int kind, int transposed,
-                                                           const __grid_constant__ HeatRule h, double *out,
-                                                           int64_t *st) {
+// one entry of the stiffness block from S_pq = V (k grad lam_p) . grad lam_q
+// and the rule's tables (i, j compile-time after unrolling)
+__device__ __forceinline__ double exact_stiff(const double (&S)[4][4], const HeatRule &h, int i, int j) {
+  constexpr int A[6] = {0, 0, 0, 1, 1, 2}, B[6] = {1, 2, 3, 2, 3, 3};
+  if (i < 4 && j < 4) return S[i][j] * h.kvv[i][j];
+  if (i < 4) {
+    const int a = A[j - 4], b = B[j - 4];
+    return S[i][a] * h.kve[i][b] + S[i][b] * h.kve[i][a];
+  }
+  if (j < 4) {
+    const int a = A[i - 4], b = B[i - 4];
+    return S[a][j] * h.kve[j][b] + S[b][j] * h.kve[j][a];
+  }
+  const int a = A[i - 4], b = B[i - 4], c = A[j - 4], d = B[j - 4];
+  return h.w16[b][d] * S[a][c] + h.w16[b][c] * S[a][d] + h.w16[a][d] * S[b][c] + h.w16[a][c] * S[b][d];
+}
+
+// KIND 0 stiffness, 1 capacity; TR 1 writes each tet's block transposed. The
+// 100 values of a tet are staged in two halves of 50 (13.2 KB per warp; the
+// stiffness kernel at 126 registers), so 16 one-warp CTAs share an SM.
+// Quarters, for 32 capacity CTAs per SM, measured 1.9x slower.
+template <int KIND, int TR>
+__global__ void __launch_bounds__(kExactTets, 16) k_leg2_exact(const double *nodes, int64_t nN, const int32_t *tets,
+                                                               int64_t nT, const double *coef,
+                                                               const __grid_constant__ HeatRule h, double *out,
+                                                               int64_t *st) {
   constexpr int LD = kExactTets + 1;  // padded: the coalesced read walks values of one tet
-  __shared__ double stage[100 * LD];
+  constexpr int PART = 50;
+  __shared__ double stage[PART * LD];
   const int tl = threadIdx.x;
   const int64_t t0 = (int64_t)blockIdx.x * kExactTets, t = t0 + tl;
   double X[4][3];
@@ -392,12 +415,11 @@ __global__ void __launch_bounds__(kExactTets) k_leg2_exact(const double *nodes, 
     ok = idx_ok && V > 0.0 && isfinite(V);
     if (!ok) flag(st, idx_ok ? EMG_ST_DEGENERATE : EMG_ST_INDEX, t);
   }
-  if (kind == 1) {
-    const double rv = ok ? coef[t] * V : 0.0;
-#pragma unroll
-    for (int k = 0; k < 100; ++k) stage[k * LD + tl] = h.c[k] * rv;  // C symmetric: both layouts
+  double S[4][4];
+  double rv = 0.0;
+  if constexpr (KIND == 1) {
+    rv = ok ? coef[t] * V : 0.0;
   } else {
-    double S[4][4];
     if (ok) {
       const double inv = 1.0 / det;
       for (int p = 1; p < 4; ++p)
@@ -419,34 +441,25 @@ __global__ void __launch_bounds__(kExactTets) k_leg2_exact(const double *nodes, 
 #pragma unroll
         for (int q = 0; q < 4; ++q) S[p][q] = 0.0;
     }
-    constexpr int A[6] = {0, 0, 0, 1, 1, 2}, B[6] = {1, 2, 3, 2, 3, 3};
-#pragma unroll
-    for (int i = 0; i < 10; ++i)
-#pragma unroll
-      for (int j = 0; j < 10; ++j) {
-        double v;
-        if (i < 4 && j < 4) {
-          v = S[i][j] * h.kvv[i][j];
-        } else if (i < 4) {
-          const int a = A[j - 4], b = B[j - 4];
-          v = S[i][a] * h.kve[i][b] + S[i][b] * h.kve[i][a];
-        } else if (j < 4) {
-          const int a = A[i - 4], b = B[i - 4];
-          v = S[a][j] * h.kve[j][b] + S[b][j] * h.kve[j][a];
-        } else {
-          const int a = A[i - 4], b = B[i - 4], c = A[j - 4], d = B[j - 4];
-          v = h.w16[b][d] * S[a][c] + h.w16[b][c] * S[a][d] + h.w16[a][d] * S[b][c] + h.w16[a][c] * S[b][d];
-        }
-        stage[(transposed ? 10 * j + i : 10 * i + j) * LD + tl] = v;
-      }
   }
-  __syncthreads();
-  // value-major stage -> the block's contiguous output
-  const int64_t n = min((int64_t)kExactTets, nT - t0) * 100;
+  const int64_t nt = min((int64_t)kExactTets, nT - t0);
   double *o = out + t0 * 100;
-  for (int k = tl; k < n; k += kExactTets) {
-    const int tt = k / 100, e = k - tt * 100;
-    o[k] = stage[e * LD + tt];
+#pragma unroll
+  for (int part = 0; part < 100 / PART; ++part) {
+    // output position o_k = 10 r + c of the stored block; (i, j) is (r, c),
+    // or (c, r) when the block is stored transposed
+#pragma unroll
+    for (int q = 0; q < PART; ++q) {
+      const int ok_ = part * PART + q, r = ok_ / 10, c = ok_ % 10;
+      const int i = TR ? c : r, j = TR ? r : c;
+      stage[q * LD + tl] = KIND == 1 ? h.c[10 * i + j] * rv : exact_stiff(S, h, i, j);
+    }
+    __syncthreads();
+    for (int k = tl; k < nt * PART; k += kExactTets) {
+      const int tt = k / PART, e = k - tt * PART;
+      o[(int64_t)tt * 100 + part * PART + e] = stage[e * LD + tt];
+    }
+    __syncthreads();
   }
 }
 
@@ -472,8 +485,15 @@ extern "C" int emg_leg2_element(const double *d_nodes, int64_t n_nodes, const in
   if (precision == EMG_EXACT) {
     static const HeatRule rule = make_heat_rule();
     const int64_t blocks = (n_tets + kExactTets - 1) / kExactTets;
-    k_leg2_exact<<<(unsigned)blocks, kExactTets, 0, s>>>(d_nodes, n_nodes, d_tets, n_tets, d_coef, kind, tr, rule,
-                                                        d_values, d_status);
+#define EMG_EX(K, T) \
+  k_leg2_exact<K, T><<<(unsigned)blocks, kExactTets, 0, s>>>(d_nodes, n_nodes, d_tets, n_tets, d_coef, rule, d_values, \
+                                                             d_status)
+    if (kind == 1) {
+      if (tr) EMG_EX(1, 1); else EMG_EX(1, 0);
+    } else {
+      if (tr) EMG_EX(0, 1); else EMG_EX(0, 0);
+    }
+#undef EMG_EX
     return launch_check("k_leg2_exact");
   }
   // prefer shared memory over L1 for the fp64 kernels, once per device (a
