@@ -1043,7 +1043,7 @@ def run_serving(args, rank, world, local_rank):
                        "alloc_conf": os.environ.get("PYTORCH_CUDA_ALLOC_CONF", ""),
                        "parallelism": f"replicas x{world}"},
             "serving": r, "clocks": r["clocks"]}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = CpuServingBaseline(jobs).measure()
     return line if rank == 0 else None
 
@@ -1079,7 +1079,9 @@ def main():
         line, wl = run_heat(args, rank, world, local_rank)
     else:
         line, wl = run_ours(args, rank, world, local_rank)
-    if rank == 0 and not args.no_cpu_baseline and wl is not None:
+    # the host-core baseline is taken at N = 1 only (rank 0), so that N > 1
+    # runs hold their GPUs for the GPU work alone
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and wl is not None:
         if args.sweep and args.sweep_conductive:
             cb = CpuBaseline(wl, args.cpu_sample_tets).measure()  # the reference reassembles every frequency
             cb["value"] /= wl.field.ntets
