@@ -135,8 +135,19 @@ __constant__ SecondSlotTable kSecondSlot = make_second_slot_table();
 // off each position's chain, with the register count held for six CTAs per
 // SM. Complex64 values keep the plain loop (32 registers and eight CTAs per SM
 // with 8-byte records), where the prefetch measured slower.
+// Warps per CTA and CTAs per SM. A warp's time follows its chunk's list
+// lengths, and a CTA's slot frees only when its slowest warp ends, so small
+// CTAs keep more warps resident: 4-warp CTAs, 12 per SM at 40 registers
+// (complex128) or 16 at 32 (complex64). Compact records keep 8-warp CTAs.
 template <typename R, bool COMPACT>
-__global__ void __launch_bounds__(PG_WARPS * 32, (std::is_same<R, double>::value || COMPACT) ? 6 : 8)
+struct PackedShape {
+  static constexpr bool c128 = std::is_same<R, double>::value;
+  static constexpr int warps = !COMPACT ? 4 : PG_WARPS;
+  static constexpr int min_blocks = (c128 && !COMPACT) ? 12 : (!COMPACT ? 16 : 6);
+};
+
+template <typename R, bool COMPACT>
+__global__ void __launch_bounds__(PackedShape<R, COMPACT>::warps * 32, PackedShape<R, COMPACT>::min_blocks)
     k_gather_packed(const int32_t *ent_ptr, const int32_t *order, const void *pidx_v, const uint16_t *posoff,
                     int64_t E, int64_t F, int64_t n_values, const int32_t *indptr, const void *v, double ar,
                     double ai, double2 *A) {
@@ -147,7 +158,9 @@ __global__ void __launch_bounds__(PG_WARPS * 32, (std::is_same<R, double>::value
   }
   const int lane = threadIdx.x & 31;
   ChunkMeta m;
-  if (!chunk_meta(ent_ptr, order, indptr, E, F, (int64_t)blockIdx.x * PG_WARPS + (threadIdx.x >> 5), m)) return;
+  if (!chunk_meta(ent_ptr, order, indptr, E, F,
+                  (int64_t)blockIdx.x * PackedShape<R, COMPACT>::warps + (threadIdx.x >> 5), m))
+    return;
   const int total = 20 * (m.I1 - m.I0);
   constexpr bool PREFETCH = std::is_same<R, double>::value;
   int n0 = 0, n1 = 0;
@@ -303,9 +316,10 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
     const void *pidx = plan + p->off_pidx;
     const int64_t nv = p->n_assy * 210;
     const bool compact = p->record_bytes == 4;
-#define EMG_PK(R, C)                                                                                             \
-  k_gather_packed<R, C><<<g, PG_WARPS * 32, 0, s>>>(ent_ptr, order, pidx, posoff, p->n_edges, p->n_tris, nv, d_indptr, \
-                                                    d_v1, ar, ai, A)
+#define EMG_PK(R, C)                                                                                    \
+  k_gather_packed<R, C><<<grid_for(n_chunks(p->n_edges, p->n_tris), PackedShape<R, C>::warps),           \
+                          PackedShape<R, C>::warps * 32, 0, s>>>(ent_ptr, order, pidx, posoff, p->n_edges,  \
+                                                                 p->n_tris, nv, d_indptr, d_v1, ar, ai, A)
     if (f32) {
       if (compact) EMG_PK(float, true); else EMG_PK(float, false);
     } else {
