@@ -5,8 +5,6 @@
 // e.g. a plugin running inside another framework's pre-reserved device pool,
 // or a latency-bound loop that must not call cudaMalloc/cudaFree (cudaFree
 // synchronises the whole device). They still pass inputs and outputs.
-#include <mutex>
-
 #include "common.cuh"
 
 namespace emg {
@@ -18,23 +16,15 @@ namespace {
 constexpr size_t kStaticValuesBytes = size_t(96) << 20;
 static __device__ __align__(256) unsigned char g_static_values[kStaticValuesBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void *g_addr[kMaxDevices] = {};
-
-// device address of g_static_values on the current device (looked up once per
-// device; the host-side name is only a stand-in, never a device address)
+// Device address of g_static_values in the current device's context. Looked
+// up on every call: the lookup is a host-side table read once the module is
+// loaded, and a cached address would go stale when the caller resets the
+// device (cudaDeviceReset unloads the module; the next lookup loads it
+// again). The host-side name is only a stand-in, never a device address.
 int static_values_address(void **out) {
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return fail(EMG_EDEVICE, "device ordinal %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    CUDA_TRY(cudaGetSymbolAddress(&p, g_static_values));
-    g_addr[dev] = p;
-  }
-  *out = g_addr[dev];
+  void *p = nullptr;
+  CUDA_TRY(cudaGetSymbolAddress(&p, g_static_values));
+  *out = p;
   return EMG_OK;
 }
 

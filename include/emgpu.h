@@ -228,8 +228,10 @@ int emg_assemble(const emg_plan *plan, const void *d_plan, const int32_t *d_indp
  * device array of 96 MiB that every GPU loading this library holds until
  * exit: at most 29,959 assembled tets in EMG_FP64/EMG_EXACT, 59,918 in
  * EMG_MIXED; larger plans return EMG_ERANGE. It calls no cudaMalloc/cudaFree.
- * The first call on a device looks the array's address up on that device
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call looks the array's address up in the current device's context
+ * (cudaGetSymbolAddress), so a device reset between calls is safe; the
+ * first call on a device loads the module there, so make that first call
+ * before any stream capture.
  * All calls share the array: calls that overlap on the GPU (other streams or
  * threads) race and corrupt each other's results. Inputs and outputs are the
  * caller's, as for emg_assemble. */
