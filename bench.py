@@ -39,7 +39,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="wr90_dielectric", choices=["wr90_dielectric", "wr90_air"])
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-sample-tets", type=int, default=200000)
+    ap.add_argument("--cpu-sample-tets", type=int, default=200000,
+                    help="tets of the bounded CPU samples of the --sweep / --pml / --heat / --shard modes")
+    ap.add_argument("--cpu-chunk-tets", type=int, default=100000,
+                    help="tets per chunk of the reference arm's whole-workload assembly")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="hex grid nx,ny,nz of the dielectric box (default 100,50,67)")
     ap.add_argument("--forms", default="fp64,mixed", help="comma list of forms to time (fp64, mixed, exact)")
@@ -218,27 +221,78 @@ class CpuSweepBaseline(CpuBaseline):
                 "sample": self.desc}
 
 
+def arm_config(wl, nnz):
+    """The workload both arms run (the same dict in both lines)."""
+    return {"workload": wl.name, "tets": int(wl.n_tets), "hex_grid": list(wl.hex_grid), "nnz": int(nnz),
+            "N": int(wl.field.n_field), "freq_hz": wl.freq, "assembled": "A = K - k0^2 M values, pattern cached"}
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU algorithm (oracle port) on the
-    host cores, same metric/unit/config; rank 0 only."""
+    """--impl reference: the reference's CPU algorithm (the C port of its
+    _matrix_builder + to_csc in oracle/) on all host threads, over the WHOLE
+    workload every step: the assembled tets in chunks of --cpu-chunk-tets,
+    each chunk's element matrices built and scattered into the one CSC value
+    array in the reference scatter's order (bit for bit the one-piece
+    result; the full COO, 19.2 KB per tet, would not fit in host memory).
+    The pattern and the chunks' scatter orders are built once before the
+    timed steps, as the reference caches its CSCMapping. Rank 0 only."""
     if rank != 0:
         return None
+    from oracle import oracle as O
+
     wl = make_workload(args.config, grid=args.grid)
-    cb = CpuBaseline(wl, args.cpu_sample_tets)
+    t0 = time.perf_counter()
+    ca = O.ChunkedAssembly(wl.field, wl.er, wl.ur, wl.conductor_tets, chunk_tets=args.cpu_chunk_tets)
+    setup_s = time.perf_counter() - t0
+    out = np.zeros(ca.nnz, np.complex128)
+    beta = -wl.k0 ** 2
     for _ in range(args.warmup):
-        cb.step()
-    ts = [cb.step() for _ in range(args.steps)]
-    v = cb.n / float(np.median(ts))
-    ms = 1e3 * wl.n_tets / v
+        ca.step(1.0, beta, out)
+    ts = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        ca.step(1.0, beta, out)
+        ts.append(time.perf_counter() - t1)
+    mean_s = float(np.mean(ts))
+    v = wl.n_tets / mean_s
+    desc = (f"the whole {wl.name} workload ({wl.n_tets} tets) every step: element build (_matrix_builder) + "
+            f"scatter of E - k0^2 B into A in the reference's order, {len(ca.chunks)} chunks of "
+            f"<= {ca.chunk_tets} tets, {ca.nthreads} threads, pattern cached")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": 1e3 * mean_s, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": wl.name, "tets": wl.n_tets, "hex_grid": list(wl.hex_grid),
-                       "freq_hz": wl.freq, "sample_per_step": cb.desc,
-                       "ms_per_step_note": "extrapolated from the sample rate to the full workload"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb.cores, "kind": "port", "sample": cb.desc},
+            "config": arm_config(wl, ca.nnz),
+            "reference_setup_s": setup_s, "step_s": {"min": min(ts), "median": float(np.median(ts)),
+                                                     "max": max(ts)},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ca.nthreads, "kind": "port", "sample": desc},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
+
+
+def cpu_baseline_subprocess(args):
+    """The reference arm (whole workload, all host threads) in a fresh
+    process: 1 warm-up and 2 timed steps. A fresh process keeps the CPU
+    timing apart from this process's GPU-side threads, pinned buffers and
+    OpenMP runtimes, so both CPU numbers of a run come from the same code in
+    the same conditions."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "2", "--warmup", "1",
+           "--config", args.config, "--cpu-chunk-tets", str(args.cpu_chunk_tets)]
+    if args.grid:
+        cmd += ["--grid", args.grid]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=1200, env=env)
+    except subprocess.TimeoutExpired:
+        return {"value": None, "unavailable": "reference arm timed out"}
+    for ln in reversed(r.stdout.strip().splitlines()):
+        try:
+            d = json.loads(ln)
+        except ValueError:
+            continue
+        cb = dict(d["cpu_baseline"])
+        cb["sample"] += "; run as `bench.py --impl reference --steps 2 --warmup 1` in a fresh process"
+        return cb
+    return {"value": None, "unavailable": f"reference arm failed (rc {r.returncode}): {r.stderr[-300:]}"}
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -437,12 +491,11 @@ def run_ours(args, rank, world, local_rank):
             del v64, v32
         cmap._ws = None
         dmesh.check_status()
-    # e2e through the public API (host numpy in, host scipy out), mixed form
-    e2e = None
-    if args.e2e_steps > 0:
+    # e2e through the public API (host numpy in, host scipy out), both forms
+    def e2e_run(precision):
         nodes_b = f.mesh.nodes.nbytes
         tets_b = f.mesh.tets.shape[1] * 4 * 4
-        E, B, _ = tet_mass_stiffness_matrices(f, wl.er, wl.ur, wl.conductor_tets, cmap, precision="mixed",
+        E, B, _ = tet_mass_stiffness_matrices(f, wl.er, wl.ur, wl.conductor_tets, cmap, precision=precision,
                                               device=dev)
         A = cmap.to_csc(E - B * k0 ** 2)  # warm
         # the mapping's device tets are reused when the same tet array comes back
@@ -453,7 +506,7 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            E, B, _ = tet_mass_stiffness_matrices(f, wl.er, wl.ur, wl.conductor_tets, cmap, precision="mixed",
+            E, B, _ = tet_mass_stiffness_matrices(f, wl.er, wl.ur, wl.conductor_tets, cmap, precision=precision,
                                                   device=dev)
             A = cmap.to_csc(E - B * k0 ** 2)
             times.append(time.perf_counter() - t0)
@@ -463,11 +516,17 @@ def run_ours(args, rank, world, local_rank):
             tt = torch.tensor([t], device=dev)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             t = float(tt.item())
-        e2e = {"value": world * f.ntets / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(cmap.nnz * 16), "s_per_step": t,
-               "path": "tet_mass_stiffness_matrices(..., cscmap) + GpuCSCMapping.to_csc(E - B*k0**2) -> scipy "
-                       "csc_matrix; per step: node coordinates and materials copied in, A copied out"
-                       + ("; tets resident in the mapping" if tets_shared else "")}
+        return {"value": world * f.ntets / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(cmap.nnz * 16), "s_per_step": t, "form": precision,
+                "path": "tet_mass_stiffness_matrices(..., cscmap, precision) + GpuCSCMapping.to_csc(E - B*k0**2) "
+                        "-> scipy csc_matrix; per step: node coordinates and materials copied in, A copied out"
+                        + ("; tets resident in the mapping" if tets_shared else "")}
+
+    e2e = e2e_fp64 = None
+    if args.e2e_steps > 0:
+        e2e = e2e_run("mixed")
+        e2e_fp64 = e2e_run("fp64")
+        cmap._ws = None
     line = None
     if rank == 0:
         nT, nnz, nN = f.ntets, cmap.nnz, f.mesh.n_nodes
@@ -486,6 +545,12 @@ def run_ours(args, rank, world, local_rank):
         traffic = load_traffic(wl.name) or {}
 
         def roof(r, form):
+            """Roofline of the dominant kernel (the gather) on the algorithmic
+            bytes of one assembly step: nodes, tets, materials, the int32
+            slot -> nonzero map (400 per tet), the segment offsets and A written
+            (balg, 7,187 B per tet here) over the gather's CUDA-event time. The
+            kernels' own algorithmic bytes -- which count the element values'
+            round trip through HBM -- are kept beside it."""
             vb = 8 if form == "mixed" else 16
             kb = {"k_element": W.element_alg_bytes(nN, nT, vb, 16), "k_gather": W.gather_alg_bytes(nT, nnz, vb)}
             kms = {"k_element": r["k_element_ms"], "k_gather": r["k_gather_ms"]}
@@ -493,13 +558,15 @@ def run_ours(args, rank, world, local_rank):
             kern = {}
             for k in kb:
                 ach = kb[k] / (kms[k] * 1e-3) / 1e9
-                kern[k] = {"alg_bytes": kb[k], "ms": kms[k], "achieved": ach, "frac": ach / hbm,
+                kern[k] = {"own_alg_bytes": kb[k], "ms": kms[k], "own_achieved": ach, "own_frac": ach / hbm,
                            "traffic": traffic.get(f"{form}_{k}_bytes")}
+            ach = balg / (kms[dom] * 1e-3) / 1e9
             step_ach = balg / (r["ms"] * 1e-3) / 1e9
-            d = kern[dom]
-            return {"bound": "hbm", "kernel": dom, "achieved": d["achieved"], "peak": hbm, "unit": "GB/s",
-                    "frac": d["frac"], "traffic": d["traffic"], "peak_source": peak_src,
-                    "alg_bytes_per_launch": d["alg_bytes"], "kernels": kern,
+            return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                    "frac": ach / hbm, "traffic": kern[dom]["traffic"], "peak_source": peak_src,
+                    "alg_bytes_per_launch": balg,
+                    "alg_bytes_rule": "24 nN + 16 nT + 16 nT (er) + 4 x 400 nT + 4 (nnz + 1) + 16 nnz",
+                    "kernels": kern,
                     "step": {"alg_bytes": balg, "achieved": step_ach, "frac": step_ach / hbm,
                              "floor_bytes": bfloor, "floor_frac": bfloor / (r["ms"] * 1e-3) / 1e9 / hbm,
                              "traffic": traffic.get(f"{form}_step_bytes")}}
@@ -508,18 +575,19 @@ def run_ours(args, rank, world, local_rank):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": mx["ms"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64 geometry + f32 contraction (mixed), f64 sum", "data": "synthetic",
-                "config": {"workload": wl.name, "tets": nT, "hex_grid": list(wl.hex_grid), "nnz": nnz,
-                           "N": f.n_field, "freq_hz": wl.freq, "form": primary,
-                           "l2": mx["l2"],
-                           "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
-                           "alg_bytes_per_step": balg, "floor_bytes_per_step": bfloor,
-                           "plan_build_s": plan_s},
+                "config": arm_config(wl, nnz),
+                "form": primary, "l2": mx["l2"],
+                "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
+                "alg_bytes_per_step": balg, "floor_bytes_per_step": bfloor, "plan_build_s": plan_s,
                 "plain_fp64": {"value": world * nT / (fp["ms"] * 1e-3), "ms_per_step": fp["ms"],
                                "k_element_ms": fp["k_element_ms"], "k_gather_ms": fp["k_gather_ms"],
-                               "gather_record_bytes": fp["record_bytes"], "roofline": roof(fp, "fp64")},
+                               "gather_record_bytes": fp["record_bytes"], "roofline": roof(fp, "fp64"),
+                               "e2e": e2e_fp64},
                 "mixed": {"k_element_ms": mx["k_element_ms"], "k_gather_ms": mx["k_gather_ms"]},
                 "mixed_over_plain": fp["ms"] / mx["ms"], "mixed_vs_fp64_errors": errors,
-                "roofline": roof(mx, primary), "clocks": mx["clocks"], "e2e": e2e, "gpu_launches": 2 * args.steps}
+                "roofline": roof(mx, primary), "clocks": mx["clocks"], "e2e": e2e,
+                # per timed step: the status-word reset, the element kernel and the gather
+                "gpu_launches": 3 * args.steps}
     return line, wl
 
 
@@ -1089,9 +1157,11 @@ def main():
             cb["sample"] += "; per frequency, scaled to the full mesh by tet count (reassembly, as the reference "\
                             "does for conductive materials)"
             line["cpu_baseline"] = cb
-        else:
+        elif args.heat or args.sweep or args.pml:
             base = HeatCpuBaseline if args.heat else (CpuSweepBaseline if args.sweep else CpuBaseline)
             line["cpu_baseline"] = base(wl, args.cpu_sample_tets).measure()
+        else:
+            line["cpu_baseline"] = cpu_baseline_subprocess(args)
     if world > 1:
         import torch.distributed as dist
 

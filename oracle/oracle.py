@@ -17,6 +17,10 @@ surface on numpy arrays:
 * ``tri_force``, ``force_entries``, ``tri_points`` -> robinbc.py:104-135,220-313
                           (``generate_points_3d``, ``ned2_tri_force``,
                           ``compute_force_entries``)
+* ``ChunkedAssembly``  -> _matrix_builder + to_csc(E - k0^2 B) (curlcurl.py:387-456,
+                          csc_cast.py:55-177, assembler.py:494) over all tets of a
+                          mesh too large for its full COO, in chunks of tets, equal
+                          bit for bit to the one-piece scatter (chunked_oracle.c)
 * ``topology_loops``   -> mesh3d.py:706-776 and nedelec2.py:61-79 restated as
   plain Python loops (small meshes only; checks the vectorised host topology)
 
@@ -88,6 +92,16 @@ def lib():
         L.oracle_port_overlap.restype = None
         L.oracle_port_overlap.argtypes = [_p, _i64, _p, _i64, _p, _i64, _p, _i64, _p, _p, _p, _p, _p, _i64, _p,
                                           ctypes.c_int, _p, ctypes.c_double, _p, _p]
+        L.oracle_dof_incidence.restype = ctypes.c_int
+        L.oracle_dof_incidence.argtypes = [_p, _i64, _p, _i64, _i64, _p, _p]
+        L.oracle_pattern_rows.restype = _i64
+        L.oracle_pattern_rows.argtypes = [_p, _i64, _p, _p, _p, _i64, _i64, _p, _p, ctypes.c_int]
+        L.oracle_chunk_order.restype = ctypes.c_int
+        L.oracle_chunk_order.argtypes = [_p, _i64, _p, _i64, _i64, _p, _p, _i64, _p, _p, _p, ctypes.c_int,
+                                         ctypes.c_int]
+        L.oracle_chunk_scatter.restype = None
+        L.oracle_chunk_scatter.argtypes = [_p, _p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double, _p, _p, _p, ctypes.c_int, _p, ctypes.c_int]
         L.oracle_force_entries.restype = ctypes.c_int
         L.oracle_force_entries.argtypes = [_p, _i64, _p, _i64, _p, _p, _i64, _p, _i64, _p]
         _lib = L
@@ -127,6 +141,102 @@ def matrix_builder(nodes, tets, tris, edges, tet_to_field, tet_to_edge, tet_to_t
     if rc != 0:
         raise ValueError("tet id out of range")
     return dataE, dataB, rows, cols
+
+
+def matrix_builder_into(mesh_arrays, tetids, out, nthreads: int = 0):
+    """``_matrix_builder`` (curlcurl.py:387-456) into preallocated arrays:
+    mesh_arrays = (nodes, tets, tris, edges, t2f, t2e, t2t, ur, er) already
+    contiguous in the oracle's dtypes, out = (dataE, dataB, rows, cols) of at
+    least 400 * len(tetids) entries."""
+    nodes, tets, tris, edges, t2f, t2e, t2t, ur, er = mesh_arrays
+    dataE, dataB, rows, cols = out
+    nA = tetids.shape[0]
+    rc = lib().oracle_matrix_builder(_ptr(nodes), nodes.shape[1], _ptr(tets), tets.shape[1], _ptr(tris),
+                                     tris.shape[1], _ptr(edges), edges.shape[1], _ptr(t2f), _ptr(t2e), _ptr(t2t),
+                                     _ptr(ur), _ptr(er), _ptr(tetids), nA, _ptr(dataE), _ptr(dataB), _ptr(rows),
+                                     _ptr(cols), int(nthreads))
+    if rc != 0:
+        raise ValueError("tet id out of range")
+
+
+class ChunkedAssembly:
+    """The reference's cached-pattern assembly of A = E - k0^2 B over every
+    assembled tet of a mesh whose full COO arrays (19.2 KB per tet) would not
+    fit in host memory: ``_matrix_builder`` on chunks of consecutive tetids,
+    each chunk scattered into the one CSC value array in the order of the
+    reference's ``to_csc`` (column, row, slot), so the result equals the
+    one-piece ``CSCPattern.values_lincomb`` bit for bit (chunked_oracle.c).
+    The pattern and each chunk's scatter order are built once (the reference
+    caches its CSCMapping); ``step`` is the per-frequency work."""
+
+    def __init__(self, field, er, ur, conductor_tets, chunk_tets: int = 100_000, nthreads: int = 0):
+        mesh = field.mesh
+        self.nthreads = int(nthreads) if nthreads else num_threads()
+        nT = mesh.tets.shape[1]
+        tet_assy = np.arange(nT, dtype=np.int64)
+        conductor_tets = np.asarray(conductor_tets, dtype=np.int64)
+        if conductor_tets.size:
+            tet_assy = np.delete(tet_assy, conductor_tets)
+        self.tetids = np.ascontiguousarray(tet_assy)
+        self.nA = nA = self.tetids.shape[0]
+        self.N = N = int(field.n_field)
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        i64 = lambda a: np.ascontiguousarray(a, dtype=np.int64)
+        c16 = lambda a: np.ascontiguousarray(a, dtype=np.complex128)
+        self.mesh_arrays = (f64(mesh.nodes), i64(mesh.tets), i64(mesh.tris), i64(mesh.edges),
+                            i64(field.get_tet_to_field()), i64(mesh.tet_to_edge), i64(mesh.tet_to_tri), c16(ur),
+                            c16(er))
+        t2f = self.mesh_arrays[4]
+        L = lib()
+        dptr = np.empty(N + 1, np.int64)
+        dtet = np.empty(20 * nA, np.int32)
+        if L.oracle_dof_incidence(_ptr(t2f), nT, _ptr(self.tetids), nA, N, _ptr(dptr), _ptr(dtet)) != 0:
+            raise ValueError("DoF index out of range")
+        max_deg = int(np.diff(dptr).max()) if N else 0
+        self.indptr = np.empty(N + 1, np.int64)
+        nnz = L.oracle_pattern_rows(_ptr(t2f), nT, _ptr(self.tetids), _ptr(dptr), _ptr(dtet), N, max_deg,
+                                    _ptr(self.indptr), None, self.nthreads)
+        if nnz < 0:
+            raise MemoryError("pattern rows")
+        self.nnz = int(nnz)
+        self.indices = np.empty(self.nnz, np.int32)
+        L.oracle_pattern_rows(_ptr(t2f), nT, _ptr(self.tetids), _ptr(dptr), _ptr(dtet), N, max_deg,
+                              _ptr(self.indptr), _ptr(self.indices), self.nthreads)
+        del dptr, dtet
+        self.chunk_tets = int(chunk_tets)
+        self.chunks = []
+        nsplit = 4 * self.nthreads
+        for a0 in range(0, nA, self.chunk_tets):
+            a1 = min(nA, a0 + self.chunk_tets)
+            S = 400 * (a1 - a0)
+            perm = np.empty(S, np.int32)
+            tgt = np.empty(S, np.int32)
+            splits = np.empty(nsplit + 1, np.int64)
+            rc = L.oracle_chunk_order(_ptr(t2f), nT, _ptr(self.tetids), a0, a1, _ptr(self.indptr),
+                                      _ptr(self.indices), N, _ptr(perm), _ptr(tgt), _ptr(splits), nsplit,
+                                      self.nthreads)
+            if rc != 0:
+                raise ValueError(f"chunk order failed ({rc})")
+            self.chunks.append((a0, a1, perm, tgt, splits))
+        n = min(self.chunk_tets, nA) if nA else 1
+        self.buf = (np.empty(400 * n, np.complex128), np.empty(400 * n, np.complex128), np.empty(400 * n, np.int64),
+                    np.empty(400 * n, np.int64))
+
+    def step(self, alpha, beta, out: np.ndarray | None = None) -> np.ndarray:
+        """A's values (complex128 [nnz], CSC order): alpha*E + beta*B over all
+        assembled tets, chunk by chunk."""
+        a, b = complex(alpha), complex(beta)
+        if out is None:
+            out = np.zeros(self.nnz, np.complex128)
+        else:
+            out[:] = 0
+        L = lib()
+        dE, dB = self.buf[0], self.buf[1]
+        for a0, a1, perm, tgt, splits in self.chunks:
+            matrix_builder_into(self.mesh_arrays, self.tetids[a0:a1], self.buf, self.nthreads)
+            L.oracle_chunk_scatter(_ptr(dE), _ptr(dB), a.real, a.imag, b.real, b.imag, _ptr(perm), _ptr(tgt),
+                                   _ptr(splits), splits.shape[0] - 1, _ptr(out), self.nthreads)
+        return out
 
 
 class CSCPattern:

@@ -1,6 +1,7 @@
 """`bench.py --impl reference` (the reference's CPU algorithm, timed on the
-host cores) keeps the benchmark line's contract; it needs no GPU, so it runs
-here on a tiny grid. Under torchrun only rank 0 works and prints."""
+host cores over the whole workload every step) keeps the benchmark line's
+contract and describes the same workload as the GPU arm; it needs no GPU,
+so it runs here on a tiny grid. Under torchrun only rank 0 works and prints."""
 import json
 import os
 import subprocess
@@ -27,6 +28,12 @@ def test_reference_line_contract():
     assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
     assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 2 and d["warmup"] == 1
     assert d["config"]["tets"] == 6 * 3 * 4 * 6 and d["config"]["workload"] == "wr90_dielectric"
+    wl = bench.make_workload("wr90_dielectric", grid="6,3,4")
+    m = wl.field.mesh
+    nnz = 4 * m.n_edges + 52 * m.n_tris + 168 * m.n_tets
+    assert d["config"] == json.loads(json.dumps(bench.arm_config(wl, nnz)))  # the GPU arm's config dict
+    assert abs(d["ms_per_step"] * 1e-3 * d["value"] - d["config"]["tets"]) <= 1e-6 * d["config"]["tets"]
+    assert "whole" in d["cpu_baseline"]["sample"]
     cb = d["cpu_baseline"]
     assert set(cb) >= {"value", "unit", "cores", "kind", "sample"} and cb["kind"] == "port"
     assert cb["value"] == d["value"] and cb["cores"] >= 1
