@@ -65,7 +65,9 @@ def parse():
                          "after another and timed (an estimate of N-GPU strong scaling, not a measurement of it)")
     ap.add_argument("--serving", action="store_true",
                     help="serving stream instead: Poisson arrivals of assembly jobs (5k-500k tets, 1-64 frequencies)")
-    ap.add_argument("--serving-jobs", type=int, default=50)
+    ap.add_argument("--serving-jobs", type=int, default=1000)
+    ap.add_argument("--no-serving", action="store_true",
+                    help="leave the serving stream out of the default line (it runs at N = 1)")
     ap.add_argument("--serving-rate", type=float, default=50.0, help="mean arrivals per second")
     ap.add_argument("--serving-budget-gb", type=float, default=120.0)
     ap.add_argument("--serving-workers", type=int, default=3, help="setup worker threads")
@@ -1056,8 +1058,9 @@ class CpuServingBaseline:
         for j in self.jobs:
             f = j.field
             m = f.mesh
+            er, ur = j.tensors()
             dE, dB, rows, cols = O.matrix_builder(m.nodes, m.tets, m.tris, m.edges, f.get_tet_to_field(),
-                                                  m.tet_to_edge, m.tet_to_tri, j.ur, j.er,
+                                                  m.tet_to_edge, m.tet_to_tri, ur, er,
                                                   np.arange(f.ntets, dtype=np.int64), nthreads=self.cores)
             pat = O.CSCPattern.from_rowcol(rows, cols, f.n_field, self.cores)
             del rows, cols
@@ -1076,9 +1079,10 @@ class CpuServingBaseline:
                           f"pattern and per-frequency scatter ({tf} tet-frequencies in {dt:.1f} s)"}
 
 
-def run_serving(args, rank, world, local_rank):
-    """Serving stream on this rank's GPU (replicas under torchrun: each rank
-    serves its own seeded stream). Throughput in tet-frequencies/s."""
+def serving_stream(args, rank, local_rank, budget_gb=None):
+    """One seeded serving stream on this GPU (mixed form): a short warm-up
+    stream, then --serving-jobs Poisson arrivals at --serving-rate; returns
+    the stream summary (throughput, latency percentiles, clocks) and jobs."""
     import torch
 
     from emerge_b200.serving import AssemblyServer, run_stream, synthetic_stream
@@ -1086,15 +1090,25 @@ def run_serving(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     jobs, arr = synthetic_stream(args.serving_jobs, args.serving_rate, seed=rank)
     warm, warr = synthetic_stream(3, 1000.0, tets=(5_000, 50_000), n_freq=(1, 4), seed=1000 + rank)
-    with AssemblyServer(device=local_rank, budget_bytes=args.serving_budget_gb * 1e9, precision="mixed",
+    budget = (budget_gb if budget_gb is not None else args.serving_budget_gb) * 1e9
+    with AssemblyServer(device=local_rank, budget_bytes=budget, precision="mixed",
                         setup_workers=args.serving_workers, max_batch_nnz=int(args.serving_batch_nnz)) as srv:
         run_stream(srv, warm, warr)
-        srv.n_batches = srv.n_items = 0
+        srv.drop_mesh_cache()  # the measured stream starts cold
+        srv.n_batches = srv.n_items = srv.n_km_batches = srv.n_mesh_builds = 0
         srv.peak_in_use = 0
         sampler = ClockSampler(local_rank)
         with sampler:
             r = run_stream(srv, jobs, arr)
     r["clocks"] = sampler.summary()
+    r["budget_gb"] = budget / 1e9
+    return r, jobs
+
+
+def run_serving(args, rank, world, local_rank):
+    """Serving stream on this rank's GPU (replicas under torchrun: each rank
+    serves its own seeded stream). Throughput in tet-frequencies/s."""
+    r, jobs = serving_stream(args, rank, local_rank)
     if world > 1:
         import torch.distributed as dist
 
@@ -1147,6 +1161,17 @@ def main():
         line, wl = run_heat(args, rank, world, local_rank)
     else:
         line, wl = run_ours(args, rank, world, local_rank)
+        if world == 1 and not args.no_serving:
+            # the serving stream beside the assembly line (N = 1 only)
+            import gc
+
+            import torch
+
+            gc.collect()
+            torch.cuda.empty_cache()
+            r, _ = serving_stream(args, rank, local_rank, budget_gb=min(args.serving_budget_gb, 100.0))
+            line["serving"] = {"metric": "tet-frequencies/s and job latency (arrival -> last A(f) ready)",
+                               "rate_per_s": args.serving_rate, **r}
     # the host-core baseline is taken at N = 1 only (rank 0), so that N > 1
     # runs hold their GPUs for the GPU work alone
     if rank == 0 and world == 1 and not args.no_cpu_baseline and wl is not None:

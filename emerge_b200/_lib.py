@@ -24,7 +24,8 @@ EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_material_classify", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
-    "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_abc2_build", "emg_robin_apply", "emg_robin_force",
+    "emg_plan_set_record_width", "emg_assemble_batch_table_bytes", "emg_assemble_batch",
+    "emg_robin_init", "emg_robin_build", "emg_abc2_build", "emg_robin_apply", "emg_robin_force",
     "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values", "emg_ned2_interp",
     "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol", "emg_coo_build", "emg_coo_finish", "emg_coo_gather",
     "emg_leg2_element",
@@ -85,6 +86,15 @@ class Material(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("d_er", ctypes.c_void_p), ("d_ur", ctypes.c_void_p)]
 
 
+class AssemblyJobDesc(ctypes.Structure):
+    """emg_assembly_job: one job of emg_assemble_batch."""
+    _fields_ = [("plan", ctypes.POINTER(Plan)), ("d_plan", ctypes.c_void_p), ("d_indptr", ctypes.c_void_p),
+                ("d_nodes", ctypes.c_void_p), ("n_nodes", ctypes.c_int64), ("d_tets", ctypes.c_void_p),
+                ("d_tetids", ctypes.c_void_p), ("mat", Material), ("alpha_re", ctypes.c_double),
+                ("alpha_im", ctypes.c_double), ("beta_re", ctypes.c_double), ("beta_im", ctypes.c_double),
+                ("d_values", ctypes.c_void_p), ("d_A", ctypes.c_void_p), ("d_status", ctypes.c_void_p)]
+
+
 _lib = None
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
@@ -118,6 +128,10 @@ def lib():
     L.emg_assemble_workspace_size.restype = ctypes.c_size_t
     L.emg_assemble.argtypes = [ctypes.POINTER(Plan), _P, _P, _P, _I64, _P, _P, ctypes.POINTER(Material),
                                ctypes.c_int, _D, _D, _D, _D, _P, ctypes.c_size_t, _P, _P, _P]
+    L.emg_assemble_batch_table_bytes.argtypes = [ctypes.c_int]
+    L.emg_assemble_batch_table_bytes.restype = ctypes.c_size_t
+    L.emg_assemble_batch.argtypes = [ctypes.POINTER(AssemblyJobDesc), ctypes.c_int, ctypes.c_int, _P, _P,
+                                     ctypes.c_size_t, _P]
     L.emg_form_sweep.argtypes = [_P, _P, _P, _I64, ctypes.POINTER(_D), ctypes.c_int, _P, _I64, _P]
     L.emg_form_batch.argtypes = [_P, _P, _P, ctypes.c_int, _P]
     L.emg_plan_set_record_width.argtypes = [ctypes.POINTER(Plan), ctypes.c_int]
@@ -149,7 +163,8 @@ def lib():
                                        ctypes.c_int, _D, _D, _D, _D, _P, _P, _P]
     for name in ("emg_device_check", "emg_material_classify", "emg_status_reset", "emg_status_read", "emg_plan_init", "emg_plan_build",
                  "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble", "emg_form_sweep",
-                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_robin_init", "emg_robin_build", "emg_abc2_build",
+                 "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order", "emg_plan_set_record_width", "emg_assemble_batch",
+                 "emg_robin_init", "emg_robin_build", "emg_abc2_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
                  "emg_select_values", "emg_ned2_interp", "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol",
                  "emg_coo_build", "emg_coo_finish", "emg_coo_gather", "emg_leg2_element"):

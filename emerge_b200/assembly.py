@@ -173,10 +173,23 @@ def material_kind(t: np.ndarray) -> tuple:
 
 
 class DeviceMaterial:
-    """Per-tet er, ur in the compact layout of their kind (see emg_material)."""
+    """Per-tet er, ur in the compact layout of their kind (see emg_material).
 
-    def __init__(self, er: np.ndarray, ur: np.ndarray, n_tets: int, device, alloc=None):
+    er, ur: the reference's c16[3, 3, nT] tensors, or (for callers that hold
+    isotropic materials only, such as a serving request) er as c16[nT]
+    scalars with ur None (mu_r = 1) or c16[nT]."""
+
+    def __init__(self, er: np.ndarray, ur: np.ndarray | None, n_tets: int, device, alloc=None):
         er = np.asarray(er)
+        if er.ndim == 1:
+            if er.shape != (n_tets,) or (ur is not None and np.shape(ur) != (n_tets,)):
+                raise ValueError(f"scalar er/ur must have shape ({n_tets},)")
+            self.kind = L.EMG_MAT_ISO
+            self.er = _to_dev(er.astype(np.complex128, copy=False), torch.complex128, device, alloc)
+            self.ur = (None if ur is None
+                       else _to_dev(np.asarray(ur).astype(np.complex128, copy=False), torch.complex128, device, alloc))
+            self.h2d_bytes = self.er.numel() * 16 + (self.ur.numel() * 16 if self.ur is not None else 0)
+            return
         ur = np.asarray(ur)
         if er.shape != (3, 3, n_tets) or ur.shape != (3, 3, n_tets):
             raise ValueError(f"er/ur must have shape (3, 3, {n_tets})")

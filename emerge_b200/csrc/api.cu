@@ -24,6 +24,31 @@ const char *last_error() { return g_err; }
 namespace {
 __global__ void k_probe() {}
 
+int launch_element_batch(const ElemArgs *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total, int kind,
+                         int precision, cudaStream_t s) {
+  switch (precision * 3 + kind) {
+    case 0: return launch_element_batch_0_0(d_jobs, d_cta_start, n_jobs, total, s);
+    case 1: return launch_element_batch_0_1(d_jobs, d_cta_start, n_jobs, total, s);
+    case 2: return launch_element_batch_0_2(d_jobs, d_cta_start, n_jobs, total, s);
+    case 3: return launch_element_batch_1_0(d_jobs, d_cta_start, n_jobs, total, s);
+    case 4: return launch_element_batch_1_1(d_jobs, d_cta_start, n_jobs, total, s);
+    case 5: return launch_element_batch_1_2(d_jobs, d_cta_start, n_jobs, total, s);
+    case 6: return launch_element_batch_2_0(d_jobs, d_cta_start, n_jobs, total, s);
+    case 7: return launch_element_batch_2_1(d_jobs, d_cta_start, n_jobs, total, s);
+    case 8: return launch_element_batch_2_2(d_jobs, d_cta_start, n_jobs, total, s);
+  }
+  return fail(EMG_EINVAL, "bad precision %d or kind %d", precision, kind);
+}
+
+// table layout of emg_assemble_batch: ElemArgs[n] | int64 cta[n+1] | GatherJob[n] | int64 gcta[n+1]
+size_t batch_offset(int n, int part) {
+  size_t o = 0;
+  const size_t sizes[4] = {sizeof(ElemArgs) * (size_t)n, sizeof(int64_t) * (size_t)(n + 1),
+                           sizeof(GatherJob) * (size_t)n, sizeof(int64_t) * (size_t)(n + 1)};
+  for (int i = 0; i < part; ++i) o = align_up(o + sizes[i], 16);
+  return o;
+}
+
 int launch_element(const ElemArgs &a, int kind, int precision, int layout, cudaStream_t s) {
   if (kind < EMG_MAT_ISO || kind > EMG_MAT_FULL) return fail(EMG_EINVAL, "bad material kind %d", kind);
   switch (precision * 3 + kind) {
@@ -228,6 +253,47 @@ int emg_assemble(const emg_plan *p, const void *d_plan, const int32_t *d_indptr,
   if (rc) return rc;
   return emg_gather(p, d_plan, d_indptr, d_ws, nullptr, precision, EMG_LAYOUT_PACKED, 1.0, 0.0, 0.0, 0.0, d_A,
                     d_status, stream);
+}
+
+size_t emg_assemble_batch_table_bytes(int n_jobs) { return n_jobs < 0 ? 0 : batch_offset(n_jobs, 4); }
+
+int emg_assemble_batch(const emg_assembly_job *h_jobs, int n_jobs, int precision, void *h_table, void *d_table,
+                       size_t table_bytes, emg_stream_t stream) {
+  if (n_jobs < 0 || (n_jobs > 0 && (!h_jobs || !h_table || !d_table))) return fail(EMG_EINVAL, "null pointer");
+  if (precision < EMG_FP64 || precision > EMG_EXACT) return fail(EMG_EINVAL, "bad precision %d", precision);
+  if (n_jobs == 0) return EMG_OK;
+  if (table_bytes < batch_offset(n_jobs, 4)) return fail(EMG_EINVAL, "table too small");
+  char *h = static_cast<char *>(h_table);
+  ElemArgs *ea = reinterpret_cast<ElemArgs *>(h + batch_offset(n_jobs, 0));
+  int64_t *ecta = reinterpret_cast<int64_t *>(h + batch_offset(n_jobs, 1));
+  GatherJob *ga = reinterpret_cast<GatherJob *>(h + batch_offset(n_jobs, 2));
+  int64_t *gcta = reinterpret_cast<int64_t *>(h + batch_offset(n_jobs, 3));
+  const int kind = h_jobs[0].mat.kind;
+  ecta[0] = gcta[0] = 0;
+  for (int i = 0; i < n_jobs; ++i) {
+    const emg_assembly_job &j = h_jobs[i];
+    const emg_plan *p = j.plan;
+    if (!p || !j.d_plan || !j.d_indptr || !j.mat.d_er) return fail(EMG_EINVAL, "job %d: null pointer", i);
+    if (j.mat.kind != kind) return fail(EMG_EINVAL, "job %d: material kind %d differs from %d", i, j.mat.kind, kind);
+    if (p->n_assy > 0 && (!j.d_nodes || !j.d_tets || !j.d_values || !j.d_A))
+      return fail(EMG_EINVAL, "job %d: null pointer", i);
+    if (p->n_assy < p->n_tets && !j.d_tetids) return fail(EMG_EINVAL, "job %d: tetids required", i);
+    ea[i] = ElemArgs{j.d_nodes, j.n_nodes, j.d_tets, p->n_tets, j.d_tetids, p->n_assy, j.mat.d_er, j.mat.d_ur,
+                     j.alpha_re, j.alpha_im, j.beta_re, j.beta_im, j.d_values, j.d_status};
+    ecta[i + 1] = ecta[i] + (p->n_assy + 127) / 128;
+    int rc = gather_job_fill(p, j.d_plan, j.d_indptr, j.d_values, j.d_A, &ga[i]);
+    if (rc) return rc;
+    gcta[i + 1] = gcta[i] + (p->n_ent > 0 ? ga[i].n_ctas : 0);
+  }
+  CUDA_TRY(cudaMemcpyAsync(d_table, h_table, batch_offset(n_jobs, 4), cudaMemcpyHostToDevice, S(stream)));
+  const char *d = static_cast<const char *>(d_table);
+  int rc = launch_element_batch(reinterpret_cast<const ElemArgs *>(d + batch_offset(n_jobs, 0)),
+                                reinterpret_cast<const int64_t *>(d + batch_offset(n_jobs, 1)), n_jobs,
+                                ecta[n_jobs], kind, precision, S(stream));
+  if (rc) return rc;
+  return launch_gather_batch(reinterpret_cast<const GatherJob *>(d + batch_offset(n_jobs, 2)),
+                             reinterpret_cast<const int64_t *>(d + batch_offset(n_jobs, 3)), n_jobs, gcta[n_jobs],
+                             precision, S(stream));
 }
 
 int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,

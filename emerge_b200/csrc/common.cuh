@@ -125,6 +125,17 @@ struct ElemArgs {
   int64_t *st;
 };
 
+// one job of a batched packed gather (emg_gather_batch)
+struct GatherJob {
+  const int32_t *ent_ptr, *order;
+  const void *pidx;
+  const uint16_t *posoff;
+  const int32_t *indptr;
+  const void *values;
+  double2 *A;
+  int64_t E, F, n_values, n_ctas;
+};
+
 // Gather chunks: a warp owns CHUNK consecutive entities of one kind. Their
 // items are contiguous in the plan and their first-DoF (second-DoF) columns
 // are consecutive, so each chunk's output is two contiguous runs of A.
@@ -167,6 +178,19 @@ EMG_DECLARE_ELEM(2, 0)
 EMG_DECLARE_ELEM(2, 1)
 EMG_DECLARE_ELEM(2, 2)
 
+#define EMG_DECLARE_ELEM_BATCH(F, K)                                                                      \
+  int launch_element_batch_##F##_##K(const ElemArgs *d_jobs, const int64_t *d_cta_start, int n_jobs, \
+                                     int64_t total_ctas, cudaStream_t s);
+EMG_DECLARE_ELEM_BATCH(0, 0)
+EMG_DECLARE_ELEM_BATCH(0, 1)
+EMG_DECLARE_ELEM_BATCH(0, 2)
+EMG_DECLARE_ELEM_BATCH(1, 0)
+EMG_DECLARE_ELEM_BATCH(1, 1)
+EMG_DECLARE_ELEM_BATCH(1, 2)
+EMG_DECLARE_ELEM_BATCH(2, 0)
+EMG_DECLARE_ELEM_BATCH(2, 1)
+EMG_DECLARE_ELEM_BATCH(2, 2)
+
 // element values are complex64 for the mixed form, complex128 otherwise
 inline bool values_fp32(int precision) { return precision == EMG_MIXED; }
 
@@ -197,6 +221,10 @@ int status_reset(int64_t *st, cudaStream_t s);
 int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *indptr, const void *v1, const void *v2,
                   int precision, int layout, double ar, double ai, double br, double bi, void *A, int64_t *st,
                   cudaStream_t s);
+int gather_job_fill(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_values, void *d_A,
+                    GatherJob *out);
+int launch_gather_batch(const GatherJob *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total_ctas,
+                        int precision, cudaStream_t s);
 int launch_form_sweep(const void *K, const void *M, const void *P, int64_t nnz, const double *coef, int nf,
                       void *out, int64_t stride, cudaStream_t s);
 int launch_form_batch(const emg_form_item *items, const int64_t *tile_start, const int32_t *n_items, int max_items,

@@ -666,15 +666,16 @@ __device__ __forceinline__ void all_rows_packed(const Tensors<KIND, R> &T, const
 //           computed in both of its rows);
 // LAYOUT 1: the packed canonical upper triangle [ia][210] (the assembly
 //           path, each unique entry computed once)
+// One CTA's 128 tets, assembled indices ia0 .. ia0 + 127 of the job a (every
+// thread of the CTA calls it with the same ia0).
 template <int FORM, int KIND, int LAYOUT>
-__global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
+__device__ __forceinline__ void element_cta(const ElemArgs &a, int64_t ia0, unsigned char *stage_raw) {
   using R = typename FormReal<FORM>::T;
   using ST = typename StoreT<R>::T;
   constexpr int STAGE = 20;  // values per lane
-  extern __shared__ __align__(16) unsigned char stage_raw[];
   ST *stage = reinterpret_cast<ST *>(stage_raw) + (threadIdx.x >> 5) * (32 * STAGE);
   ST *out = reinterpret_cast<ST *>(a.out);
-  const int64_t ia64 = (int64_t)blockIdx.x * ELEM_THREADS + threadIdx.x;
+  const int64_t ia64 = ia0 + threadIdx.x;
   bool active = ia64 < a.nA;
   const int ia = (int)ia64;
   Geo G;
@@ -752,6 +753,30 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
 }
 
 template <int FORM, int KIND, int LAYOUT>
+__global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  element_cta<FORM, KIND, LAYOUT>(a, (int64_t)blockIdx.x * ELEM_THREADS, stage_raw);
+}
+
+// Several jobs (meshes, materials, coefficients, outputs) in one launch of
+// the packed form: job j owns the CTAs [cta_start[j], cta_start[j + 1]) and
+// its tets in CTA order, as if launched alone.
+template <int FORM, int KIND>
+__global__ void __launch_bounds__(ELEM_THREADS) k_element_batch(const ElemArgs *jobs, const int64_t *cta_start,
+                                                                int n_jobs) {
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  const int64_t b = blockIdx.x;
+  int lo = 0, hi = n_jobs - 1;  // the job with cta_start[j] <= b < cta_start[j + 1]
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cta_start[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  if (n_jobs <= 0 || b >= cta_start[n_jobs]) return;
+  element_cta<FORM, KIND, 1>(jobs[lo], (b - cta_start[lo]) * ELEM_THREADS, stage_raw);
+}
+
+template <int FORM, int KIND, int LAYOUT>
 int launch_element_t(const ElemArgs &a, cudaStream_t s) {
   using ST = typename StoreT<typename FormReal<FORM>::T>::T;
   constexpr size_t smem = (size_t)ELEM_WARPS * 32 * 20 * sizeof(ST);
@@ -769,6 +794,26 @@ int launch_element_t(const ElemArgs &a, cudaStream_t s) {
   if (a.nA == 0) return EMG_OK;
   k_element<FORM, KIND, LAYOUT><<<grid_for(a.nA, ELEM_THREADS), ELEM_THREADS, smem, s>>>(a);
   return launch_check("k_element");
+}
+
+template <int FORM, int KIND>
+int launch_element_batch_t(const ElemArgs *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total_ctas,
+                           cudaStream_t s) {
+  using ST = typename StoreT<typename FormReal<FORM>::T>::T;
+  constexpr size_t smem = (size_t)ELEM_WARPS * 32 * 20 * sizeof(ST);
+  static bool configured[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+  if (dev >= 64 || !configured[dev]) {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_element_batch<FORM, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(EMG_ECUDA, "cudaFuncSetAttribute(k_element_batch): %s", cudaGetErrorString(e));
+    if (dev < 64) configured[dev] = true;
+  }
+  if (n_jobs == 0 || total_ctas == 0) return EMG_OK;
+  if (total_ctas > INT32_MAX) return fail(EMG_ERANGE, "too many CTAs (%lld)", (long long)total_ctas);
+  k_element_batch<FORM, KIND><<<(unsigned)total_ctas, ELEM_THREADS, smem, s>>>(d_jobs, d_cta_start, n_jobs);
+  return launch_check("k_element_batch");
 }
 
 template <int FORM, int KIND>

@@ -146,21 +146,12 @@ struct PackedShape {
   static constexpr int min_blocks = (c128 && !COMPACT) ? 12 : (!COMPACT ? 16 : 6);
 };
 
+// One warp's chunk of the packed gather (chunk meta already read).
 template <typename R, bool COMPACT>
-__global__ void __launch_bounds__(PackedShape<R, COMPACT>::warps * 32, PackedShape<R, COMPACT>::min_blocks)
-    k_gather_packed(const int32_t *ent_ptr, const int32_t *order, const void *pidx_v, const uint16_t *posoff,
-                    int64_t E, int64_t F, int64_t n_values, const int32_t *indptr, const void *v, double ar,
-                    double ai, double2 *A) {
-  __shared__ uint8_t slot2[2][210];
-  if constexpr (COMPACT) {
-    for (int i = threadIdx.x; i < 420; i += blockDim.x) slot2[i / 210][i % 210] = kSecondSlot.v[i / 210][i % 210];
-    __syncthreads();
-  }
+__device__ __forceinline__ void gather_packed_chunk(const ChunkMeta &m, const void *pidx_v, const uint16_t *posoff,
+                                                    int64_t n_values, const void *v, double ar, double ai,
+                                                    double2 *A, const uint8_t (*slot2)[210]) {
   const int lane = threadIdx.x & 31;
-  ChunkMeta m;
-  if (!chunk_meta(ent_ptr, order, indptr, E, F,
-                  (int64_t)blockIdx.x * PackedShape<R, COMPACT>::warps + (threadIdx.x >> 5), m))
-    return;
   const int total = 20 * (m.I1 - m.I0);
   constexpr bool PREFETCH = std::is_same<R, double>::value;
   int n0 = 0, n1 = 0;
@@ -205,6 +196,46 @@ __global__ void __launch_bounds__(PackedShape<R, COMPACT>::warps * 32, PackedSha
     A[m.A0 + p] = make_double2(ar * s0r - ai * s0i, ar * s0i + ai * s0r);
     A[m.A1 + p] = make_double2(ar * s1r - ai * s1i, ar * s1i + ai * s1r);
   }
+}
+
+
+template <typename R, bool COMPACT>
+__global__ void __launch_bounds__(PackedShape<R, COMPACT>::warps * 32, PackedShape<R, COMPACT>::min_blocks)
+    k_gather_packed(const int32_t *ent_ptr, const int32_t *order, const void *pidx_v, const uint16_t *posoff,
+                    int64_t E, int64_t F, int64_t n_values, const int32_t *indptr, const void *v, double ar,
+                    double ai, double2 *A) {
+  __shared__ uint8_t slot2[2][210];
+  if constexpr (COMPACT) {
+    for (int i = threadIdx.x; i < 420; i += blockDim.x) slot2[i / 210][i % 210] = kSecondSlot.v[i / 210][i % 210];
+    __syncthreads();
+  }
+  ChunkMeta m;
+  if (!chunk_meta(ent_ptr, order, indptr, E, F,
+                  (int64_t)blockIdx.x * PackedShape<R, COMPACT>::warps + (threadIdx.x >> 5), m))
+    return;
+  gather_packed_chunk<R, COMPACT>(m, pidx_v, posoff, n_values, v, ar, ai, A, slot2);
+}
+
+// Several jobs' packed gathers (8-byte records, alpha = 1) in one launch: job
+// j owns the CTAs [cta_start[j], cta_start[j + 1]) and its chunks in CTA
+// order, as if launched alone.
+template <typename R>
+__global__ void __launch_bounds__(PackedShape<R, false>::warps * 32, PackedShape<R, false>::min_blocks)
+    k_gather_packed_batch(const GatherJob *jobs, const int64_t *cta_start, int n_jobs) {
+  const int64_t b = blockIdx.x;
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cta_start[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  if (n_jobs <= 0 || b >= cta_start[n_jobs]) return;
+  const GatherJob &j = jobs[lo];
+  ChunkMeta m;
+  if (!chunk_meta(j.ent_ptr, j.order, j.indptr, j.E, j.F,
+                  (b - cta_start[lo]) * PackedShape<R, false>::warps + (threadIdx.x >> 5), m))
+    return;
+  gather_packed_chunk<R, false>(m, j.pidx, j.posoff, j.n_values, j.values, 1.0, 0.0, j.A, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -338,6 +369,39 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
   }
 #undef EMG_COO
   return launch_check("k_gather_coo");
+}
+
+int gather_job_fill(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_values, void *d_A,
+                    GatherJob *out) {
+  if (p->record_bytes != 8) return fail(EMG_EINVAL, "batched gathers take plans with 8-byte records");
+  const char *plan = static_cast<const char *>(d_plan);
+  out->ent_ptr = reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr);
+  out->order = reinterpret_cast<const int32_t *>(plan + p->off_order);
+  out->pidx = plan + p->off_pidx;
+  out->posoff = reinterpret_cast<const uint16_t *>(plan + p->off_posoff);
+  out->indptr = d_indptr;
+  out->values = d_values;
+  out->A = static_cast<double2 *>(d_A);
+  out->E = p->n_edges;
+  out->F = p->n_tris;
+  out->n_values = p->n_assy * 210;
+  out->n_ctas = (n_chunks(p->n_edges, p->n_tris) + PackedShape<double, false>::warps - 1) /
+                PackedShape<double, false>::warps;
+  return EMG_OK;
+}
+
+int launch_gather_batch(const GatherJob *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total_ctas,
+                        int precision, cudaStream_t s) {
+  if (n_jobs == 0 || total_ctas == 0) return EMG_OK;
+  if (total_ctas > INT32_MAX) return fail(EMG_ERANGE, "too many CTAs (%lld)", (long long)total_ctas);
+  static_assert(PackedShape<double, false>::warps == PackedShape<float, false>::warps, "same chunks per CTA");
+  if (values_fp32(precision))
+    k_gather_packed_batch<float><<<(unsigned)total_ctas, PackedShape<float, false>::warps * 32, 0, s>>>(
+        d_jobs, d_cta_start, n_jobs);
+  else
+    k_gather_packed_batch<double><<<(unsigned)total_ctas, PackedShape<double, false>::warps * 32, 0, s>>>(
+        d_jobs, d_cta_start, n_jobs);
+  return launch_check("k_gather_packed_batch");
 }
 
 int launch_form_batch(const emg_form_item *items, const int64_t *tile_start, const int32_t *n_items, int max_items,

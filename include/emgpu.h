@@ -220,6 +220,43 @@ int emg_assemble(const emg_plan *plan, const void *d_plan, const int32_t *d_indp
                  int precision, double alpha_re, double alpha_im, double beta_re, double beta_im, void *d_workspace,
                  size_t workspace_bytes, void *d_A, int64_t *d_status, emg_stream_t stream);
 
+/* One job of emg_assemble_batch: the arguments of emg_assemble for one mesh.
+ * d_values: that job's element-value workspace (emg_assemble_workspace_size
+ * bytes for its n_assy), d_A: its nnz complex128 values; d_status may be
+ * shared between jobs or NULL. */
+typedef struct {
+  const emg_plan *plan; /* host struct, read during the call */
+  const void *d_plan;
+  const int32_t *d_indptr;
+  const double *d_nodes;
+  int64_t n_nodes;
+  const int32_t *d_tets;
+  const int32_t *d_tetids;
+  emg_material mat;
+  double alpha_re, alpha_im, beta_re, beta_im;
+  void *d_values;
+  void *d_A;
+  int64_t *d_status;
+} emg_assembly_job;
+
+/* Bytes of the job table of emg_assemble_batch for n_jobs jobs (the same
+ * size on the host and on the device). */
+size_t emg_assemble_batch_table_bytes(int n_jobs);
+
+/* emg_assemble for n_jobs independent jobs in two launches: one element
+ * kernel over all the jobs' tets, then one packed gather over all their
+ * entity chunks (each CTA looks its job up in the table). Every job's A is
+ * bit for bit what emg_assemble gives it alone. All jobs share one material
+ * kind and the precision; their plans use 8-byte gather records. The table
+ * is written to h_table (host, emg_assemble_batch_table_bytes) and copied to
+ * d_table on the stream: when h_table is page-locked the copy is
+ * asynchronous and h_table must stay untouched until the stream has passed
+ * this call. No counterpart in the reference (batching of independent
+ * assembly jobs, a serving optimisation: a serving loop assembles K and M of
+ * every job admitted since its last launch together). */
+int emg_assemble_batch(const emg_assembly_job *h_jobs, int n_jobs, int precision, void *h_table, void *d_table,
+                       size_t table_bytes, emg_stream_t stream);
+
 /* emg_assemble without a workspace argument, for callers that cannot
  * allocate device memory at the call site (a plugin inside another
  * framework's pre-reserved device pool; a latency-bound loop that must not

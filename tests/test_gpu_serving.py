@@ -74,6 +74,7 @@ def test_mix_bitwise_equal_to_alone(alone, max_items, slots, graph):
         assert srv.n_items == sum(len(j.freqs) for j in jobs)
         if max_items < 10:
             assert srv.n_batches >= sum(len(j.freqs) for j in jobs) // max_items
+        srv.drop_mesh_cache()
         assert srv.in_use == 0
     _assert_same(jobs, ref)
     s = latency_summary(jobs)
@@ -121,3 +122,23 @@ def test_mixed_precision_jobs_alone_vs_mix():
         k0 = 2 * np.pi * freqs[0] / C0
         fro, mx = rel_err(j.results[0], cmap.to_csc(E - B * k0 ** 2).data)
         assert fro <= 1e-6 and mx <= 1e-6
+
+
+def test_shared_meshes_and_batched_setup(alone):
+    """Jobs on one mesh share its resident entry (built once); results stay
+    bitwise those of the jobs run alone, and scalar materials give what the
+    reference's [3, 3, nT] tensors give."""
+    specs, ref = alone
+    with AssemblyServer(precision="fp64", budget_bytes=8e9) as srv:
+        jobs = [srv.submit(j) for j in _jobs(specs) + _jobs(specs)]
+        srv.wait(jobs, timeout=120)
+        assert srv.n_mesh_builds == len(specs)
+        assert 1 <= srv.n_km_batches <= len(jobs)
+    _assert_same(jobs[:len(specs)], ref)
+    _assert_same(jobs[len(specs):], ref)
+    wl, freqs, cond = specs[1]  # isotropic dielectric
+    scalar = AssemblyJob(wl.field, wl.er[0, 0].copy(), None, freqs, cond, keep_results=True)
+    with AssemblyServer(precision="fp64", budget_bytes=8e9) as srv:
+        srv.submit(scalar)
+        srv.wait([scalar], timeout=120)
+    _assert_same([scalar], [ref[1]])
