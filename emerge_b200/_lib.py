@@ -26,6 +26,7 @@ EXPORTS = (
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
     "emg_plan_set_record_width", "emg_assemble_batch_table_bytes", "emg_assemble_batch",
     "emg_robin_init", "emg_robin_build", "emg_abc2_build", "emg_robin_apply", "emg_robin_force",
+    "emg_robin_build_dofs", "emg_csc_lookup", "emg_csc_shift",
     "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values", "emg_ned2_interp",
     "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol", "emg_coo_build", "emg_coo_finish", "emg_coo_gather",
     "emg_leg2_element",
@@ -142,6 +143,10 @@ def lib():
     L.emg_robin_build.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P,
                                   _P]
     L.emg_robin_apply.argtypes = [ctypes.POINTER(Robin), _P, _P, _D, _D, _P, _I64, _P]
+    L.emg_robin_build_dofs.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _P, _I64, _P,
+                                       _P, _P, _P]
+    L.emg_csc_lookup.argtypes = [_P, _P, _I64, _P, _P, _I64, _P, _P]
+    L.emg_csc_shift.argtypes = [_P, _I64, ctypes.c_int, _P, _P, ctypes.c_int, _P, _P, _I64, _P, _I64, _P]
     L.emg_select_init.argtypes = [_I64, ctypes.POINTER(Select)]
     L.emg_select_build.argtypes = [ctypes.POINTER(Select), _P, _P, _P, _P, _P, _P, _P]
     L.emg_select_finish.argtypes = [ctypes.POINTER(Select), _P, _P, _P, _P, _P, _P, _P, _P]

@@ -88,8 +88,14 @@ class DeviceMesh:
         self.n_edges = int(mesh.edges.shape[1])
         self.n_tris = int(mesh.tris.shape[1])
         self.N = int(field.n_field)
-        if self.N != 2 * self.n_edges + 2 * self.n_tris:
+        self.N_volume = 2 * self.n_edges + 2 * self.n_tris
+        if self.N < self.N_volume:
             raise ValueError("only the SECOND_MIXED_VOLAKIS space (n_field = 2E + 2F) is supported")
+        if self.N > self.N_volume:
+            # a partitioned field (ThinConductor, nedelec2.py:114-172): the
+            # volume assembly keeps the map from before the split
+            # (curlcurl.py:244) and the pattern's extra columns stay empty
+            _check_volume_map(field, mesh)
         dc = np.asarray(field.dofcodes3d)
         if dc.shape != (20,) or not np.array_equal(dc, [64] * 6 + [66] * 6 + [128] * 4 + [129] * 4):
             raise ValueError(f"unsupported dofcodes {dc.tolist()} (expected SECOND_MIXED_VOLAKIS)")
@@ -133,6 +139,18 @@ class DeviceMesh:
 
     def reset_status(self):
         L.check(L.lib().emg_status_reset(L.ptr(self.status), L.stream_handle(self.device)))
+
+
+def _check_volume_map(field, mesh) -> None:
+    """get_tet_to_field() of a partitioned field must be the unsplit map
+    (rows: tet_to_edge, + E, tet_to_tri + 2E, + 2E + F)."""
+    t2f = np.asarray(field.get_tet_to_field())
+    E, F = int(mesh.edges.shape[1]), int(mesh.tris.shape[1])
+    t2e, t2t = np.asarray(mesh.tet_to_edge), np.asarray(mesh.tet_to_tri)
+    ok = (t2f.shape == (20, t2e.shape[1]) and np.array_equal(t2f[0:6], t2e) and np.array_equal(t2f[6:12], t2e + E)
+          and np.array_equal(t2f[12:16], t2t + 2 * E) and np.array_equal(t2f[16:20], t2t + 2 * E + F))
+    if not ok:
+        raise ValueError("a partitioned field must keep its unsplit tet_to_field for the volume assembly")
 
 
 def _tet_assy(nT: int, conductor_tets):
@@ -288,7 +306,7 @@ class LinComb:
 
     def _other(self, o):
         """(job, coef) of the other operand, or NotImplemented."""
-        if isinstance(o, ElemValues) or getattr(o, "_is_robin_term", False):
+        if isinstance(o, ElemValues) or getattr(o, "_is_robin_term", False) or getattr(o, "_is_opposite_term", False):
             o = o._lc()
         if not isinstance(o, LinComb):
             return NotImplemented
@@ -344,8 +362,16 @@ class LinComb:
         """(RobinTerm, gamma) pairs of the combination."""
         return [(k, complex(v)) for k, v in self.coef.items() if getattr(k, "_is_robin_term", False)]
 
+    @property
+    def opposite_terms(self) -> list:
+        """(OppositeSideTerm, gamma) pairs of the combination."""
+        return [(k, complex(v)) for k, v in self.coef.items() if getattr(k, "_is_opposite_term", False)]
+
+    def without_opposite(self) -> "LinComb":
+        return LinComb(self.job, {k: v for k, v in self.coef.items() if not getattr(k, "_is_opposite_term", False)})
+
     def __array__(self, dtype=None, copy=None):
-        if self.robin_terms:
+        if self.robin_terms or self.opposite_terms:
             raise TypeError("a combination with a boundary term has no tet COO layout; use cscmap.to_csc")
         K = np.asarray(ElemValues(self.job, "K"))
         M = np.asarray(ElemValues(self.job, "M"))
@@ -383,6 +409,8 @@ class GpuCSCMapping:
         L.check(lib.emg_plan_build(L.ctypes.byref(plan), L.ptr(m.tets), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids),
                                    L.ptr(self.d_plan), L.ptr(ws), L.ptr(self.d_indptr), L.ptr(m.status), st))
         self.nnz = int(plan.nnz)
+        if self.N > m.N_volume:  # the split DoFs' columns of a partitioned field are empty
+            self.d_indptr[m.N_volume + 1:].fill_(self.nnz)
         self.d_indices = _empty(max(self.nnz, 1), torch.int32, m.device, m.alloc)
         L.check(lib.emg_plan_finish(L.ctypes.byref(plan), L.ptr(t2e), L.ptr(t2t), L.ptr(m.tetids),
                                     L.ptr(self.d_plan), L.ptr(self.d_indptr), L.ptr(self.d_indices),
@@ -460,9 +488,11 @@ class GpuCSCMapping:
         """Values of to_csc(data) kept on the device (complex128 [nnz])."""
         if isinstance(data, ElemValues):
             data = data._lc()
-        if getattr(data, "_is_robin_term", False):
+        if getattr(data, "_is_robin_term", False) or getattr(data, "_is_opposite_term", False):
             data = data._lc()
         if isinstance(data, LinComb):
+            if data.opposite_terms:
+                raise ValueError("an opposite-side term grows the pattern: assemble through its ExtendedCSCMapping")
             if data.job is not None:
                 out = self.assemble_device(data.job, data.alpha, data.beta)
                 data.job.mesh.check_status()

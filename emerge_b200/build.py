@@ -32,7 +32,7 @@ def _nvcc() -> str:
 
 def _units():
     units = [("api", "api.cu", []), ("plan", "plan.cu", []), ("gather", "gather.cu", []),
-             ("noalloc", "noalloc.cu", []), ("robin", "robin.cu", []),
+             ("noalloc", "noalloc.cu", []), ("robin", "robin.cu", []), ("extend", "extend.cu", []),
              ("select", "select.cu", []), ("postproc", "postproc.cu", ["-fmad=false"]),
              ("coo", "coo.cu", []), ("solve", "solve.cu", []),
              ("heat", "heat.cu", ["-fmad=false"])]

@@ -192,8 +192,8 @@ __device__ __forceinline__ bool tri_load(const int32_t *tris, const int32_t *tri
 template <bool ABC2>
 __global__ void __launch_bounds__(128)
     k_robin_build(const double *nodes, int64_t nN, const int32_t *tris, const int32_t *tri_to_edge, int64_t F,
-                  int64_t E, const int32_t *btris, int64_t nb, const int32_t *indptr, const int32_t *indices,
-                  int64_t N, uint64_t *keys, double2 *vals, int64_t *st) {
+                  int64_t E, const int32_t *btris, int64_t nb, const int32_t *tri_dofs_in, const int32_t *indptr,
+                  const int32_t *indices, int64_t N, uint64_t *keys, double2 *vals, int64_t *st) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nb) return;
   uint64_t *my_keys = keys + i * 64;
@@ -237,6 +237,8 @@ __global__ void __launch_bounds__(128)
   }
   int64_t dof[8];
   tri_dofs(e, t, E, F, dof);
+  if (tri_dofs_in)  // the caller's numbering (a partitioned field's other side)
+    for (int a = 0; a < 8; ++a) dof[a] = tri_dofs_in[i * 8 + a];
   int k = 0;
   for (int a = 0; a < 8; ++a)
     for (int b = a; b < 8; ++b, ++k) {
@@ -245,7 +247,8 @@ __global__ void __launch_bounds__(128)
         const int r = pass ? b : a, c = pass ? a : b;  // slot (r, c): row dof[r] in column dof[c]
         const int slot = 8 * r + c;
         int64_t pos = -1;
-        if (dof[c] < N && dof[r] < N) pos = find_in_column(indptr, indices, dof[c], (int32_t)dof[r]);
+        if (dof[c] >= 0 && dof[r] >= 0 && dof[c] < N && dof[r] < N)
+          pos = find_in_column(indptr, indices, dof[c], (int32_t)dof[r]);
         if (pos < 0) flag(st, EMG_ST_INDEX, i);
         my_keys[slot] = pos < 0 ? ~0ull : (((uint64_t)pos << 32) | (uint64_t)(i * 64 + slot));
         my_vals[slot] = make_double2(val, 0.0);
@@ -365,24 +368,24 @@ int emg_robin_init(int64_t n_btris, emg_robin *r) {
 namespace {
 int robin_build(bool abc2, const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
                 const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
-                const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
-                int64_t *d_status, emg_stream_t stream) {
+                const int32_t *d_tri_dofs, const int32_t *d_indptr, const int32_t *d_indices, int64_t N,
+                uint64_t *d_keys, void *d_values, int64_t *d_status, emg_stream_t stream) {
   if (!r) return fail(EMG_EINVAL, "null robin descriptor");
   if (r->n_btris == 0) return EMG_OK;
   if (!d_nodes || !d_tris || !d_tri_to_edge || !d_btris || !d_indptr || !d_indices || !d_keys || !d_values)
     return fail(EMG_EINVAL, "null pointer");
-  if (n_nodes <= 0 || n_tris <= 0 || n_edges <= 0 || N != 2 * n_edges + 2 * n_tris)
-    return fail(EMG_EINVAL, "bad sizes (N must be 2 E + 2 F)");
+  if (n_nodes <= 0 || n_tris <= 0 || n_edges <= 0 || N < 2 * n_edges + 2 * n_tris || N >= (1LL << 31))
+    return fail(EMG_EINVAL, "bad sizes (N must be at least 2 E + 2 F and below 2^31)");
   cudaStream_t s = S(stream);
   auto *vals = static_cast<double2 *>(d_values);
   if (abc2)
     k_robin_build<true><<<grid_for(r->n_btris, 128), 128, 0, s>>>(
-        d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, r->n_btris, d_indptr, d_indices, N, d_keys,
-        vals, d_status);
+        d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, r->n_btris, d_tri_dofs, d_indptr, d_indices,
+        N, d_keys, vals, d_status);
   else
     k_robin_build<false><<<grid_for(r->n_btris, 128), 128, 0, s>>>(
-        d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, r->n_btris, d_indptr, d_indices, N, d_keys,
-        vals, d_status);
+        d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, r->n_btris, d_tri_dofs, d_indptr, d_indices,
+        N, d_keys, vals, d_status);
   int rc = launch_check("k_robin_build");
   if (rc) return rc;
   if (r->n_keys > r->n_slots) {
@@ -399,16 +402,25 @@ int emg_robin_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, 
                     const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
                     const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
                     int64_t *d_status, emg_stream_t stream) {
-  return robin_build(false, r, d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, d_indptr, d_indices,
-                     N, d_keys, d_values, d_status, stream);
+  return robin_build(false, r, d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, nullptr, d_indptr,
+                     d_indices, N, d_keys, d_values, d_status, stream);
+}
+
+int emg_robin_build_dofs(const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                         const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                         const int32_t *d_tri_dofs, const int32_t *d_indptr, const int32_t *d_indices, int64_t N,
+                         uint64_t *d_keys, void *d_values, int64_t *d_status, emg_stream_t stream) {
+  if (!d_tri_dofs && r && r->n_btris) return fail(EMG_EINVAL, "null triangle DoF array");
+  return robin_build(false, r, d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, d_tri_dofs, d_indptr,
+                     d_indices, N, d_keys, d_values, d_status, stream);
 }
 
 int emg_abc2_build(const emg_robin *r, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
                    const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
                    const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
                    int64_t *d_status, emg_stream_t stream) {
-  return robin_build(true, r, d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, d_indptr, d_indices,
-                     N, d_keys, d_values, d_status, stream);
+  return robin_build(true, r, d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges, d_btris, nullptr, d_indptr,
+                     d_indices, N, d_keys, d_values, d_status, stream);
 }
 
 int emg_robin_apply(const emg_robin *r, const uint64_t *d_keys, const void *d_values, double gamma_re,
@@ -430,8 +442,8 @@ int emg_robin_force(const emg_robin *r, const double *d_nodes, int64_t n_nodes, 
   if (r->n_btris == 0) return EMG_OK;
   if (!d_nodes || !d_tris || !d_tri_to_edge || !d_btris || !d_U || !d_fkeys || !d_fvalues || !d_b)
     return fail(EMG_EINVAL, "null pointer");
-  if (n_nodes <= 0 || n_tris <= 0 || n_edges <= 0 || N != 2 * n_edges + 2 * n_tris)
-    return fail(EMG_EINVAL, "bad sizes (N must be 2 E + 2 F)");
+  if (n_nodes <= 0 || n_tris <= 0 || n_edges <= 0 || N < 2 * n_edges + 2 * n_tris)
+    return fail(EMG_EINVAL, "bad sizes (N must be at least 2 E + 2 F)");
   cudaStream_t s = S(stream);
   k_robin_force<<<grid_for(r->n_btris, 128), 128, 0, s>>>(d_nodes, n_nodes, d_tris, d_tri_to_edge, n_tris, n_edges,
                                                           d_btris, r->n_btris, static_cast<const double2 *>(d_U),

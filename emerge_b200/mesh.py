@@ -102,6 +102,40 @@ class TetMesh:
     def n_tris(self) -> int:
         return self.tris.shape[1]
 
+    @property
+    def tri_to_tet(self) -> np.ndarray:
+        """i8[2, F]: the two tets of every triangle, the lower tet index first,
+        MISSING_ID where a boundary triangle has one (mesh3d.py:781-795: a
+        stable sort of the tets' face slots by triangle)."""
+        t2t = getattr(self, "_tri_to_tet", None)
+        if t2t is None:
+            nT, F = self.n_tets, self.n_tris
+            flat = self.tet_to_tri.ravel(order="F")
+            order = np.argsort(flat, kind="stable")
+            st, stet = flat[order], np.repeat(np.arange(nT, dtype=np.int64), 4)[order]
+            t2t = np.full((2, F), MISSING_ID, dtype=np.int64)
+            _, first, counts = np.unique(st, return_index=True, return_counts=True)
+            t2t[0, st[first]] = stet[first]
+            two = counts == 2
+            t2t[1, st[first[two]]] = stet[first[two] + 1]
+            self._tri_to_tet = t2t
+        return t2t
+
+    def tri_normals(self, tri_ids: np.ndarray) -> np.ndarray:
+        """f8[3, n]: the unit normal (v1 - v0) x (v2 - v0) of each triangle in
+        its sorted vertex order (mesh3d.py:1220-1240)."""
+        v = self.nodes[:, self.tris[:, tri_ids]]  # (3, 3 vertices, n)
+        n = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0], axis=0)
+        return n / np.linalg.norm(n, axis=0)
+
+
+MISSING_ID = -1234  # mesh3d.py:29: the missing second tet of a boundary triangle
+
+
+class DoFSplitError(ValueError):
+    """A surface given to ``partition_dof`` lies on the domain's exterior
+    (the reference's DoFSplitException, nedelec2.py:32, :190-195)."""
+
 
 class Nedelec2Field:
     """The parts of the reference ``Nedelec2`` (elements/nedelec2.py:36-101)
@@ -128,9 +162,76 @@ class Nedelec2Field:
         tf[6] = np.arange(F) + 2 * E
         tf[7] = np.arange(F) + 2 * E + F
         self.tri_to_field = tf
+        self.edge_to_field = np.stack([np.arange(E), np.arange(E) + E]).astype(np.int64)
+        # set by partition_dof (nedelec2.py:82-95)
+        self.tri_to_field_os: np.ndarray | None = None
+        self.edge_to_field_os: np.ndarray | None = None
+        self._tet_to_field_orig: np.ndarray | None = None
+        self._partitioned = False
+        self.split_edges = np.zeros(0, np.int64)
+        self.split_tris = np.zeros(0, np.int64)
 
     def get_tet_to_field(self) -> np.ndarray:
+        """The DoF map the curl-curl volume assembly uses: the map from before
+        ``partition_dof`` once the field is partitioned (nedelec2.py:104-107)."""
+        if self._tet_to_field_orig is not None:
+            return self._tet_to_field_orig
         return self.tet_to_field
+
+    def partition_dof(self, surfaces) -> None:
+        """Split the DoFs of internal surfaces between their two sides
+        (``Nedelec2.partition_dof`` and ``_partition_dof_face``,
+        nedelec2.py:114-245), the set-up of a ThinConductor.
+
+        ``surfaces``: a list of (tri_ids, base_normal) pairs, one per face tag
+        of the reference (``mesh.get_triangles([tag])`` and
+        ``mesh.ftag_to_normal[tag]``). Per surface: every triangle is split;
+        an edge is split when exactly two of the surface's triangles hold it;
+        each triangle's moved tet is ``tri_to_tet[1]`` when its normal
+        (``TetMesh.tri_normals``) has a positive dot product with the base
+        normal, else ``tri_to_tet[0]``. Over all surfaces the split edges and
+        triangles are sorted and numbered after the existing DoFs: edge DoF
+        ``e + i*E`` of the k-th split edge becomes ``n + k + i*nE``, face DoF
+        ``2E + t + i*F`` of the k-th split triangle ``n + 2nE + k + i*nF``
+        (n the DoF count before, nE / nF the split counts); ``n_field`` grows
+        by ``2nE + 2nF``. The moved tets' ``tet_to_field`` columns and the
+        split triangles' ``tri_to_field_os`` columns (and ``edge_to_field_os``)
+        take the new numbers; ``get_tet_to_field()`` keeps the map from
+        before. A second call does nothing, as in the reference."""
+        if self._partitioned:
+            return
+        m = self.mesh
+        E, F = m.n_edges, m.n_tris
+        if self.tri_to_field_os is None:
+            self.tri_to_field_os = self.tri_to_field.copy()
+            self.edge_to_field_os = self.edge_to_field.copy()
+            self._tet_to_field_orig = self.tet_to_field.copy()
+        t2t = m.tri_to_tet
+        tets, edges, tris = [], [], []
+        for tri_ids, normal in surfaces:
+            ids = np.asarray(tri_ids, dtype=np.int64).ravel()
+            linked = t2t[:, ids]
+            if np.any(linked == MISSING_ID):
+                raise DoFSplitError("cannot split the DoFs of a surface on the exterior of the domain")
+            count = np.bincount(m.tri_to_edge[:, ids].ravel(), minlength=E)
+            edges.append(np.flatnonzero(count == 2))
+            tris.append(ids)
+            dot = np.sum(m.tri_normals(ids) * np.asarray(normal, dtype=np.float64).reshape(3, 1), axis=0)
+            tets.append(np.where(dot > 0, linked[1], linked[0]))
+        se = np.unique(np.concatenate(edges)) if edges else np.zeros(0, np.int64)
+        st = np.unique(np.concatenate(tris)) if tris else np.zeros(0, np.int64)
+        n0, ne, nf = self.n_field, se.size, st.size
+        remap = np.arange(n0, dtype=np.int64)
+        for i in range(2):
+            remap[se + i * E] = n0 + np.arange(ne) + i * ne
+            remap[st + 2 * E + i * F] = n0 + 2 * ne + np.arange(nf) + i * nf
+        self.n_field = n0 + 2 * ne + 2 * nf
+        moved = np.unique(np.concatenate(tets)) if tets else np.zeros(0, np.int64)
+        self.tet_to_field[:, moved] = remap[self.tet_to_field[:, moved]]
+        self.tri_to_field_os[:, st] = remap[self.tri_to_field[:, st]]
+        self.edge_to_field_os[:, se] = remap[self.edge_to_field[:, se]]
+        self.split_edges, self.split_tris = se, st
+        self._partitioned = True
 
     @property
     def n_tets(self) -> int:
@@ -203,3 +304,20 @@ def plane_tris(mesh: TetMesh, axis: int, value: float, rtol: float = 1e-9) -> np
     tol = rtol * max(float(x.max() - x.min()), 1e-300)
     on = np.abs(x - value) <= tol
     return np.flatnonzero(on[mesh.tris].all(axis=0)).astype(np.int64)
+
+
+def grid_level_tris(mesh: TetMesh, dims, axis: int, level: int, lo=(0, 0, 0), hi=None) -> np.ndarray:
+    """Ids of the triangles of a ``structured_box(*dims)`` mesh whose three
+    vertices have grid index ``level`` along ``axis`` and grid indices within
+    [lo, hi] along the other axes: a (jittered) grid surface, e.g. the strip
+    of a ThinConductor inside the box (the reference takes it from a face
+    tag, mesh3d ``get_triangles``)."""
+    nx, ny, nz = dims
+    hi = (nx, ny, nz) if hi is None else hi
+    ids = np.arange(mesh.n_nodes)
+    g = np.stack([ids % (nx + 1), (ids // (nx + 1)) % (ny + 1), ids // ((nx + 1) * (ny + 1))])
+    ok = g[axis] == level
+    for a in range(3):
+        if a != axis:
+            ok &= (g[a] >= lo[a]) & (g[a] <= hi[a])
+    return np.flatnonzero(ok[mesh.tris].all(axis=0)).astype(np.int64)

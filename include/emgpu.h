@@ -346,6 +346,38 @@ int emg_robin_build(const emg_robin *robin, const double *d_nodes, int64_t n_nod
                     const int32_t *d_indptr, const int32_t *d_indices, int64_t N, uint64_t *d_keys, void *d_values,
                     int64_t *d_status, emg_stream_t stream);
 
+/* emg_robin_build with the caller's DoF numbering: d_tri_dofs (int32
+ * [n_btris][8]) gives each listed triangle's 8 DoFs in tri_to_field slot
+ * order (3 ne0 edges, 3 ne2 edges, nf0, nf1). For the opposite side of a
+ * ThinConductor these are the columns of tri_to_field_os (nedelec2.py:
+ * 156-158), and the term is field.generate_csc(B2, empty_tri_rowcol(
+ * other_side=True)) of assembler.py:605-608,636-639 (femdata.py:86-104): the
+ * same blocks on the split DoFs. d_indptr/d_indices must already hold every
+ * pair (the union pattern of emg_csc_lookup / emg_csc_shift). */
+int emg_robin_build_dofs(const emg_robin *robin, const double *d_nodes, int64_t n_nodes, const int32_t *d_tris,
+                         const int32_t *d_tri_to_edge, int64_t n_tris, int64_t n_edges, const int32_t *d_btris,
+                         const int32_t *d_tri_dofs, const int32_t *d_indptr, const int32_t *d_indices, int64_t N,
+                         uint64_t *d_keys, void *d_values, int64_t *d_status, emg_stream_t stream);
+
+/* Pattern lookup: d_out[i] = the position of (d_rows[i], d_cols[i]) (int64)
+ * in the CSC pattern d_indptr/d_indices of N columns, or -(1 + p) with p the
+ * position the row would be inserted at in its column (INT64_MIN for an
+ * index outside [0, N)). Used to lay out the union of A's pattern and extra
+ * entries (scipy's csc + csc, which the reference's K += generate_csc(...)
+ * performs, assembler.py:636-639). */
+int emg_csc_lookup(const int32_t *d_indptr, const int32_t *d_indices, int64_t N, const int64_t *d_cols,
+                   const int64_t *d_rows, int64_t n, int64_t *d_out, emg_stream_t stream);
+
+/* Shifted copy into a grown pattern: d_dst[p + d_seg_shift[s]] = d_src[p] for
+ * p < n_src, s the last segment with d_seg_start[s] <= p (d_seg_start[0] = 0,
+ * ascending, n_seg entries), then d_dst[d_xpos[e]] = d_xval[e] (zero when
+ * d_xval is NULL) for e < n_x. elem_bytes 16 (complex128 values), 8
+ * (complex64) or 4 (int32 row indices). Positions outside [0, n_dst) are
+ * skipped. One launch; HBM-bound. */
+int emg_csc_shift(const void *d_src, int64_t n_src, int elem_bytes, const int64_t *d_seg_start,
+                  const int64_t *d_seg_shift, int n_seg, const int64_t *d_xpos, const void *d_xval, int64_t n_x,
+                  void *d_dst, int64_t n_dst, emg_stream_t stream);
+
 /* The second-order absorbing boundary correction in place of the Robin
  * block, same descriptor, buffers, keys and emg_robin_apply: per triangle
  * B[a][b] = A sum_q w_q c_a c_b with c the scalar 2-D curls of the 8

@@ -396,20 +396,23 @@ def robin_entries(field, tri_ids, gamma: complex, Bmat: np.ndarray | None = None
     return Bmat
 
 
-def tri_rowcol(field):
+def tri_rowcol(field, other_side: bool = False):
     """``empty_tri_rowcol`` (femdata.py:75-92): per tri 64 slots,
-    rows[p + 8*ii + jj] = t2f[ii], cols[...] = t2f[jj] over ``tri_to_field``."""
-    t2f = field.tri_to_field  # (8, F)
+    rows[p + 8*ii + jj] = t2f[ii], cols[...] = t2f[jj] over ``tri_to_field``,
+    or over ``tri_to_field_os`` (the split DoFs of a partitioned field) with
+    ``other_side``."""
+    t2f = field.tri_to_field_os if other_side else field.tri_to_field  # (8, F)
     F = t2f.shape[1]
     rows = np.repeat(t2f.T[:, :, None], 8, axis=2).reshape(F * 64)
     cols = np.repeat(t2f.T[:, None, :], 8, axis=1).reshape(F * 64)
     return rows, cols
 
 
-def generate_csc(field, data: np.ndarray) -> csc_matrix:
-    """``generate_csc`` (femdata.py:104-118) with the tri row/col arrays:
-    the nonzero slots only, duplicates summed by scipy."""
-    rows, cols = tri_rowcol(field)
+def generate_csc(field, data: np.ndarray, rowcol=None) -> csc_matrix:
+    """``generate_csc`` (femdata.py:104-118) with the tri row/col arrays
+    (``tri_rowcol(field)`` unless given): the nonzero slots only, duplicates
+    summed by scipy, shape (n_field, n_field)."""
+    rows, cols = tri_rowcol(field) if rowcol is None else rowcol
     ids = np.argwhere(data != 0)[:, 0]
     return csc_matrix((data[ids], (rows[ids], cols[ids])), shape=(field.n_field, field.n_field))
 

@@ -87,3 +87,42 @@ def load_reference(ref_root: str = DEFAULT_REF_ROOT):
     ns.heat = importlib.import_module("emerge._emerge.physics.heatconduction.assembly.grad")
     ns.integrals = importlib.import_module("emerge._emerge.mth.integrals")
     return ns
+
+
+def _module_from_file(name: str, path: str) -> types.ModuleType:
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_nedelec2(ref_root: str = DEFAULT_REF_ROOT):
+    """The reference's Nedelec-2 basis class (``elements/nedelec2.py``, with
+    ``femdata.FEMBasis`` and ``dofsets``) for generating the partitioned-field
+    (ThinConductor) fixture. Its imports of the mesh class, the ``emsutil``
+    save mixin and the compiled interpolation library are stubbed: the
+    constructor, ``partition_dof``, ``empty_tri_rowcol`` and ``generate_csc``
+    only read the mesh object they are given. Call after ``load_reference``."""
+    em = os.path.join(ref_root, "src", "emerge", "_emerge")
+    if "emsutil" not in sys.modules:
+        try:
+            importlib.import_module("emsutil")
+        except ImportError:
+            stub = types.ModuleType("emsutil")
+            stub.Saveable = object
+            sys.modules["emsutil"] = stub
+    if "emerge._emerge.mesh3d" not in sys.modules:
+        m3 = types.ModuleType("emerge._emerge.mesh3d")
+        m3.Mesh3D = object  # a type hint only
+        sys.modules["emerge._emerge.mesh3d"] = m3
+    comp = sys.modules["emerge._emerge.compiled"]
+    if not hasattr(comp, "MATHLIB"):
+        comp.MATHLIB = None  # the interpolators are not called
+    el = os.path.join(em, "elements")
+    ns = types.SimpleNamespace()
+    ns.dofsets = _module_from_file("emerge._emerge.elements.dofsets", os.path.join(el, "dofsets.py"))
+    ns.femdata = _module_from_file("emerge._emerge.elements.femdata", os.path.join(el, "femdata.py"))
+    ns.nedelec2 = _module_from_file("emerge._emerge.elements.nedelec2", os.path.join(el, "nedelec2.py"))
+    return ns
