@@ -383,6 +383,7 @@ def kernel_times(cmap, job, prec, alpha, beta, out, reps, stream, l2=None):
     mat = job.mat.struct()
     lib = L.lib()
     h = L.ctypes.c_void_p(stream.cuda_stream)
+    layout = L.EMG_LAYOUT_BLOCK if cmap.plan.value_layout == L.EMG_LAYOUT_BLOCK else L.EMG_LAYOUT_PACKED
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     te, tg = 0.0, 0.0
     for _ in range(reps):
@@ -390,11 +391,11 @@ def kernel_times(cmap, job, prec, alpha, beta, out, reps, stream, l2=None):
             l2.flush(stream)
         ev[0].record(stream)
         L.check(lib.emg_element_values(L.ptr(m.nodes), m.n_nodes, L.ptr(m.tets), m.n_tets, L.ptr(m.tetids),
-                                       m.n_assy, L.ctypes.byref(mat), prec, L.EMG_OUT_LINCOMB, L.EMG_LAYOUT_PACKED,
+                                       m.n_assy, L.ctypes.byref(mat), prec, L.EMG_OUT_LINCOMB, layout,
                                        alpha.real, alpha.imag, beta.real, beta.imag, L.ptr(ws), None, h))
         ev[1].record(stream)
         L.check(lib.emg_gather(L.ctypes.byref(cmap.plan), L.ptr(cmap.d_plan), L.ptr(cmap.d_indptr), L.ptr(ws), None,
-                               prec, L.EMG_LAYOUT_PACKED, 1.0, 0.0, 0.0, 0.0, L.ptr(out), None, h))
+                               prec, layout, 1.0, 0.0, 0.0, 0.0, L.ptr(out), None, h))
         ev[2].record(stream)
         torch.cuda.synchronize()
         te += ev[0].elapsed_time(ev[1])
@@ -429,11 +430,10 @@ def run_ours(args, rank, world, local_rank):
     f = wl.field
     dmesh = DeviceMesh(f, wl.conductor_tets, dev)
     t0 = time.perf_counter()
-    cmap8 = GpuCSCMapping(dmesh, record_bytes=8)  # mixed form: 8-byte gather records
+    cmap0 = GpuCSCMapping(dmesh)  # entity-pair block layout: 4-byte records, four entries of A each
     torch.cuda.synchronize()
     plan_s = time.perf_counter() - t0
-    cmaps = {8: cmap8}
-    cmap = cmap8
+    cmap = cmap0
     dmat = DeviceMaterial(wl.er, wl.ur, f.ntets, dev)
     k0 = wl.k0
     alpha, beta = 1.0 + 0j, complex(-k0 ** 2)
@@ -444,10 +444,7 @@ def run_ours(args, rank, world, local_rank):
     for pname in [x for x in ("fp64", "mixed", "exact") if x in args.forms.split(",")]:
         prec = forms[pname]
         job = _Job(dmesh, dmat, prec)
-        width = 8  # 8-byte gather records for every form (the faster width for each)
-        if width not in cmaps:
-            cmaps[width] = GpuCSCMapping(dmesh, record_bytes=width)
-        cmap = cmaps[width]
+        cmap = cmap0
         cmap.workspace(prec)
         l2 = L2Guard(assembly_footprint(cmap, prec), dev)
 
@@ -470,12 +467,12 @@ def run_ours(args, rank, world, local_rank):
             ms = float(t.item())
         dmesh.check_status()
         te, tg = kernel_times(cmap, job, prec, alpha, beta, out, 3, stream, l2)
-        results[pname] = {"ms": ms, "k_element_ms": te, "k_gather_ms": tg, "record_bytes": width,
+        results[pname] = {"ms": ms, "k_element_ms": te, "k_gather_ms": tg, "value_layout": cmap.value_layout,
                           "clocks": sampler.summary() if sampler else None, "l2": l2.text()}
         del l2
         torch.cuda.synchronize()
         cmap._ws = None  # element workspace of this form
-    cmap = cmap8
+    cmap = cmap0
     # the mixed form's error against FP64 (which matches the oracle to 1e-12)
     # for K, M and A, relative Frobenius and max entry, on the device
     errors = None
@@ -554,7 +551,8 @@ def run_ours(args, rank, world, local_rank):
             kernels' own algorithmic bytes -- which count the element values'
             round trip through HBM -- are kept beside it."""
             vb = 8 if form == "mixed" else 16
-            kb = {"k_element": W.element_alg_bytes(nN, nT, vb, 16), "k_gather": W.gather_alg_bytes(nT, nnz, vb)}
+            vpt = 220 if r.get("value_layout") == "block" else 210
+            kb = {"k_element": W.element_alg_bytes(nN, nT, vb, 16, vpt), "k_gather": W.gather_alg_bytes(nT, nnz, vb, vpt)}
             kms = {"k_element": r["k_element_ms"], "k_gather": r["k_gather_ms"]}
             dom = max(kms, key=kms.get)
             kern = {}
@@ -583,7 +581,7 @@ def run_ours(args, rank, world, local_rank):
                 "alg_bytes_per_step": balg, "floor_bytes_per_step": bfloor, "plan_build_s": plan_s,
                 "plain_fp64": {"value": world * nT / (fp["ms"] * 1e-3), "ms_per_step": fp["ms"],
                                "k_element_ms": fp["k_element_ms"], "k_gather_ms": fp["k_gather_ms"],
-                               "gather_record_bytes": fp["record_bytes"], "roofline": roof(fp, "fp64"),
+                               "value_layout": fp["value_layout"], "roofline": roof(fp, "fp64"),
                                "e2e": e2e_fp64},
                 "mixed": {"k_element_ms": mx["k_element_ms"], "k_gather_ms": mx["k_gather_ms"]},
                 "mixed_over_plain": fp["ms"] / mx["ms"], "mixed_vs_fp64_errors": errors,

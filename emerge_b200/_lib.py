@@ -17,14 +17,14 @@ EMG_ST_INDEX, EMG_ST_DEGENERATE, EMG_ST_CAPACITY = 1, 2, 4
 EMG_MAT_ISO, EMG_MAT_DIAG, EMG_MAT_FULL = 0, 1, 2
 EMG_FP64, EMG_MIXED, EMG_EXACT = 0, 1, 2
 EMG_OUT_LINCOMB, EMG_OUT_K, EMG_OUT_M = 0, 1, 2
-EMG_LAYOUT_COO, EMG_LAYOUT_PACKED, EMG_LAYOUT_COO_T = 0, 1, 2
+EMG_LAYOUT_COO, EMG_LAYOUT_PACKED, EMG_LAYOUT_COO_T, EMG_LAYOUT_BLOCK = 0, 1, 2, 3
 
 # every symbol include/emgpu.h declares
 EXPORTS = (
     "emg_version", "emg_last_error", "emg_device_check", "emg_material_classify", "emg_status_reset", "emg_status_read", "emg_plan_init",
     "emg_plan_build", "emg_plan_finish", "emg_element_values", "emg_gather", "emg_assemble_workspace_size",
     "emg_assemble", "emg_form_sweep", "emg_assemble_noalloc", "emg_form_batch", "emg_plan_order",
-    "emg_plan_set_record_width", "emg_assemble_batch_table_bytes", "emg_assemble_batch",
+    "emg_plan_set_record_width", "emg_plan_set_value_layout", "emg_assemble_batch_table_bytes", "emg_assemble_batch",
     "emg_robin_init", "emg_robin_build", "emg_abc2_build", "emg_robin_apply", "emg_robin_force",
     "emg_robin_build_dofs", "emg_csc_lookup", "emg_csc_shift",
     "emg_select_init", "emg_select_build", "emg_select_finish", "emg_select_values", "emg_ned2_interp",
@@ -55,6 +55,8 @@ class Plan(ctypes.Structure):
         ("plan_bytes", ctypes.c_size_t),
         ("workspace_bytes", ctypes.c_size_t),
         ("record_bytes", ctypes.c_int32),
+        ("value_layout", ctypes.c_int32),
+        ("off_hoff", ctypes.c_size_t),
     ]
 
 
@@ -136,6 +138,7 @@ def lib():
     L.emg_form_sweep.argtypes = [_P, _P, _P, _I64, ctypes.POINTER(_D), ctypes.c_int, _P, _I64, _P]
     L.emg_form_batch.argtypes = [_P, _P, _P, ctypes.c_int, _P]
     L.emg_plan_set_record_width.argtypes = [ctypes.POINTER(Plan), ctypes.c_int]
+    L.emg_plan_set_value_layout.argtypes = [ctypes.POINTER(Plan), ctypes.c_int]
     L.emg_plan_order.argtypes = [ctypes.POINTER(Plan), _P, _P, _I64, _P, _P, _P, _P]
     L.emg_robin_init.argtypes = [_I64, ctypes.POINTER(Robin)]
     L.emg_abc2_build.argtypes = [ctypes.POINTER(Robin), _P, _I64, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P,
@@ -172,7 +175,8 @@ def lib():
                  "emg_robin_init", "emg_robin_build", "emg_abc2_build",
                  "emg_robin_apply", "emg_robin_force", "emg_select_init", "emg_select_build", "emg_select_finish",
                  "emg_select_values", "emg_ned2_interp", "emg_port_overlap", "emg_sparse_solve", "emg_coo_init", "emg_coo_rowcol",
-                 "emg_coo_build", "emg_coo_finish", "emg_coo_gather", "emg_leg2_element"):
+                 "emg_coo_build", "emg_coo_finish", "emg_coo_gather", "emg_leg2_element", "emg_plan_set_value_layout",
+                 "emg_robin_build_dofs", "emg_csc_lookup", "emg_csc_shift"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

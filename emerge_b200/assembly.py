@@ -382,11 +382,20 @@ class LinComb:
 class GpuCSCMapping:
     """The reference's ``CSCMapping`` (csc_cast.py:29-63) on the GPU: the
     sparsity pattern (indptr, indices: bit-identical to the reference's) and
-    the column-gather plan, built once per mesh and assembled-tet set."""
+    the column-gather plan, built once per mesh and assembled-tet set.
 
-    def __init__(self, dmesh: DeviceMesh, chunk_order: str = "morton", record_bytes: int = 8):
+    ``value_layout``: the element values the assembly writes and gathers --
+    ``"block"`` (default: per tet the 2x2 blocks of its 55 entity pairs, one
+    4-byte record and one contiguous read per four entries of A) or
+    ``"packed"`` (the canonical upper triangle, one record per two entries,
+    ``record_bytes`` 8 or 4). A is bit for bit the same in both."""
+
+    def __init__(self, dmesh: DeviceMesh, chunk_order: str = "morton", record_bytes: int = 8,
+                 value_layout: str = "block"):
         if chunk_order not in ("morton", "interleave"):
             raise ValueError(f"chunk_order must be 'morton' or 'interleave', got {chunk_order!r}")
+        if value_layout not in ("packed", "block"):
+            raise ValueError(f"value_layout must be 'packed' or 'block', got {value_layout!r}")
         lib = L.lib()
         m = dmesh
         self.device = m.device
@@ -399,6 +408,9 @@ class GpuCSCMapping:
         if record_bytes == 4 and m.n_assy * 210 >= (1 << 31):
             record_bytes = 8  # too many tets for the compact record
         L.check(lib.emg_plan_set_record_width(L.ctypes.byref(plan), int(record_bytes)))
+        if value_layout == "block":
+            L.check(lib.emg_plan_set_value_layout(L.ctypes.byref(plan), L.EMG_LAYOUT_BLOCK))
+        self.value_layout = value_layout
         self.plan = plan
         self.alloc = m.alloc
         self.d_plan = _empty(max(plan.plan_bytes, 1), torch.uint8, m.device, m.alloc)
@@ -543,5 +555,5 @@ def tet_mass_stiffness_matrices(field, er: np.ndarray, ur: np.ndarray, conductor
     dmat = DeviceMaterial(er, ur, dmesh.n_tets, dmesh.device)
     job = _Job(dmesh, dmat, _prec(precision))
     if cscmap is None:
-        cscmap = GpuCSCMapping(dmesh, record_bytes=8)
+        cscmap = GpuCSCMapping(dmesh)
     return ElemValues(job, "K"), ElemValues(job, "M"), cscmap

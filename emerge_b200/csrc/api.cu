@@ -25,17 +25,17 @@ namespace {
 __global__ void k_probe() {}
 
 int launch_element_batch(const ElemArgs *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total, int kind,
-                         int precision, cudaStream_t s) {
+                         int precision, int layout, cudaStream_t s) {
   switch (precision * 3 + kind) {
-    case 0: return launch_element_batch_0_0(d_jobs, d_cta_start, n_jobs, total, s);
-    case 1: return launch_element_batch_0_1(d_jobs, d_cta_start, n_jobs, total, s);
-    case 2: return launch_element_batch_0_2(d_jobs, d_cta_start, n_jobs, total, s);
-    case 3: return launch_element_batch_1_0(d_jobs, d_cta_start, n_jobs, total, s);
-    case 4: return launch_element_batch_1_1(d_jobs, d_cta_start, n_jobs, total, s);
-    case 5: return launch_element_batch_1_2(d_jobs, d_cta_start, n_jobs, total, s);
-    case 6: return launch_element_batch_2_0(d_jobs, d_cta_start, n_jobs, total, s);
-    case 7: return launch_element_batch_2_1(d_jobs, d_cta_start, n_jobs, total, s);
-    case 8: return launch_element_batch_2_2(d_jobs, d_cta_start, n_jobs, total, s);
+    case 0: return launch_element_batch_0_0(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 1: return launch_element_batch_0_1(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 2: return launch_element_batch_0_2(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 3: return launch_element_batch_1_0(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 4: return launch_element_batch_1_1(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 5: return launch_element_batch_1_2(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 6: return launch_element_batch_2_0(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 7: return launch_element_batch_2_1(d_jobs, d_cta_start, n_jobs, total, layout, s);
+    case 8: return launch_element_batch_2_2(d_jobs, d_cta_start, n_jobs, total, layout, s);
   }
   return fail(EMG_EINVAL, "bad precision %d or kind %d", precision, kind);
 }
@@ -171,6 +171,19 @@ int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tri
   p->n_items = 10 * n_assy;
   p->N = 2 * (n_edges + n_tris);
   p->record_bytes = 8;
+  p->value_layout = EMG_LAYOUT_PACKED;
+  plan_layout(p);
+  p->workspace_bytes = plan_workspace_bytes(p);
+  return EMG_OK;
+}
+
+int emg_plan_set_value_layout(emg_plan *p, int layout) {
+  if (!p) return fail(EMG_EINVAL, "null plan");
+  if (layout != EMG_LAYOUT_PACKED && layout != EMG_LAYOUT_BLOCK)
+    return fail(EMG_EINVAL, "value layout must be EMG_LAYOUT_PACKED or EMG_LAYOUT_BLOCK, got %d", layout);
+  if (layout == EMG_LAYOUT_BLOCK && !block_record_fits(p->n_assy))
+    return fail(EMG_ERANGE, "block records address at most %lld assembled tets", (long long)((1LL << 31) / 55));
+  p->value_layout = layout;
   plan_layout(p);
   p->workspace_bytes = plan_workspace_bytes(p);
   return EMG_OK;
@@ -229,7 +242,12 @@ int emg_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, c
                emg_stream_t stream) {
   if (!p || !d_plan || !d_indptr) return fail(EMG_EINVAL, "null pointer");
   if (p->nnz > 0 && (!d_v1 || !d_A)) return fail(EMG_EINVAL, "null value pointer");
-  if (layout == EMG_LAYOUT_PACKED && d_v2) return fail(EMG_EINVAL, "the packed layout takes one value array");
+  if ((layout == EMG_LAYOUT_PACKED || layout == EMG_LAYOUT_BLOCK) && d_v2)
+    return fail(EMG_EINVAL, "the packed and block layouts take one value array");
+  if (layout == EMG_LAYOUT_BLOCK && p->value_layout != EMG_LAYOUT_BLOCK)
+    return fail(EMG_EINVAL, "a block-layout gather needs a plan built with EMG_LAYOUT_BLOCK");
+  if (layout == EMG_LAYOUT_PACKED && p->value_layout != EMG_LAYOUT_PACKED)
+    return fail(EMG_EINVAL, "a packed-layout gather needs a plan built with EMG_LAYOUT_PACKED");
   return launch_gather(p, d_plan, d_indptr, d_v1, d_v2, precision, layout, ar, ai, br, bi, d_A, d_status,
                        S(stream));
 }
@@ -237,7 +255,7 @@ int emg_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, c
 size_t emg_assemble_workspace_size(int64_t n_assy, int precision) {
   if (n_assy < 0) return 0;
   if (precision < EMG_FP64 || precision > EMG_EXACT) return 0;
-  return (size_t)n_assy * 210 * (values_fp32(precision) ? 8 : 16);
+  return (size_t)n_assy * kBlockValues * (values_fp32(precision) ? 8 : 16);  // either layout (210 or 220 per tet)
 }
 
 int emg_assemble(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const double *d_nodes,
@@ -248,11 +266,12 @@ int emg_assemble(const emg_plan *p, const void *d_plan, const int32_t *d_indptr,
   if (p->n_assy > 0 && (!d_ws || ws_bytes < emg_assemble_workspace_size(p->n_assy, precision)))
     return fail(EMG_EINVAL, "workspace too small: %zu < %zu", ws_bytes,
                 emg_assemble_workspace_size(p->n_assy, precision));
+  const int layout = p->value_layout == EMG_LAYOUT_BLOCK ? EMG_LAYOUT_BLOCK : EMG_LAYOUT_PACKED;
   int rc = emg_element_values(d_nodes, n_nodes, d_tets, p->n_tets, d_tetids, p->n_assy, mat, precision,
-                              EMG_OUT_LINCOMB, EMG_LAYOUT_PACKED, ar, ai, br, bi, d_ws, d_status, stream);
+                              EMG_OUT_LINCOMB, layout, ar, ai, br, bi, d_ws, d_status, stream);
   if (rc) return rc;
-  return emg_gather(p, d_plan, d_indptr, d_ws, nullptr, precision, EMG_LAYOUT_PACKED, 1.0, 0.0, 0.0, 0.0, d_A,
-                    d_status, stream);
+  return emg_gather(p, d_plan, d_indptr, d_ws, nullptr, precision, layout, 1.0, 0.0, 0.0, 0.0, d_A, d_status,
+                    stream);
 }
 
 size_t emg_assemble_batch_table_bytes(int n_jobs) { return n_jobs < 0 ? 0 : batch_offset(n_jobs, 4); }
@@ -269,12 +288,15 @@ int emg_assemble_batch(const emg_assembly_job *h_jobs, int n_jobs, int precision
   GatherJob *ga = reinterpret_cast<GatherJob *>(h + batch_offset(n_jobs, 2));
   int64_t *gcta = reinterpret_cast<int64_t *>(h + batch_offset(n_jobs, 3));
   const int kind = h_jobs[0].mat.kind;
+  const int layout = h_jobs[0].plan ? h_jobs[0].plan->value_layout : EMG_LAYOUT_PACKED;
   ecta[0] = gcta[0] = 0;
   for (int i = 0; i < n_jobs; ++i) {
     const emg_assembly_job &j = h_jobs[i];
     const emg_plan *p = j.plan;
     if (!p || !j.d_plan || !j.d_indptr || !j.mat.d_er) return fail(EMG_EINVAL, "job %d: null pointer", i);
     if (j.mat.kind != kind) return fail(EMG_EINVAL, "job %d: material kind %d differs from %d", i, j.mat.kind, kind);
+    if (p->value_layout != layout)
+      return fail(EMG_EINVAL, "job %d: value layout %d differs from %d", i, p->value_layout, layout);
     if (p->n_assy > 0 && (!j.d_nodes || !j.d_tets || !j.d_values || !j.d_A))
       return fail(EMG_EINVAL, "job %d: null pointer", i);
     if (p->n_assy < p->n_tets && !j.d_tetids) return fail(EMG_EINVAL, "job %d: tetids required", i);
@@ -289,11 +311,11 @@ int emg_assemble_batch(const emg_assembly_job *h_jobs, int n_jobs, int precision
   const char *d = static_cast<const char *>(d_table);
   int rc = launch_element_batch(reinterpret_cast<const ElemArgs *>(d + batch_offset(n_jobs, 0)),
                                 reinterpret_cast<const int64_t *>(d + batch_offset(n_jobs, 1)), n_jobs,
-                                ecta[n_jobs], kind, precision, S(stream));
+                                ecta[n_jobs], kind, precision, layout, S(stream));
   if (rc) return rc;
   return launch_gather_batch(reinterpret_cast<const GatherJob *>(d + batch_offset(n_jobs, 2)),
                              reinterpret_cast<const int64_t *>(d + batch_offset(n_jobs, 3)), n_jobs, gcta[n_jobs],
-                             precision, S(stream));
+                             precision, layout, S(stream));
 }
 
 int emg_form_sweep(const void *d_K, const void *d_M, const void *d_P, int64_t nnz, const double *h_coef, int nf,

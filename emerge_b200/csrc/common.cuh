@@ -62,6 +62,19 @@ __host__ __device__ __forceinline__ int canon_dof(int ranks, int r) {
 // index of canonical pair (x, y), x <= y, in the packed upper triangle
 __host__ __device__ __forceinline__ int packed_index(int x, int y) { return x * (41 - x) / 2 + (y - x); }
 
+// Entity-pair block layout (EMG_LAYOUT_BLOCK): block (i, j), i <= j, of the
+// tet's canonical entities (0-5 edges, 6-9 faces) at 4 * block_index(i, j)
+// holds [(i1,j1), (i1,j2), (i2,j1), (i2,j2)] of the entities' first and second
+// canonical DoFs; 55 blocks, 220 values per tet.
+constexpr int kBlockValues = 220;
+__host__ __device__ __forceinline__ constexpr int block_index(int i, int j) { return i * (21 - i) / 2 + (j - i); }
+__host__ __device__ __forceinline__ constexpr int ent_dof1(int i) { return i < 6 ? i : 12 + (i - 6); }
+__host__ __device__ __forceinline__ constexpr int ent_dof2(int i) { return i < 6 ? i + 6 : 16 + (i - 6); }
+// Block gather record: ia * 55 + block_index(min(a, b), max(a, b)) of row
+// entity a and column entity b, bit 31 set when a > b (the block is stored
+// transposed: its middle two values swap).
+__host__ __device__ __forceinline__ bool block_record_fits(int64_t n_assy) { return n_assy * 55 < (1LL << 31); }
+
 // Compact gather record (emg_plan.record_bytes = 4; one uint32 per
 // contribution instead of an int2 of both value indices): the packed index of
 // the contribution's first-column value, ia * 210 + p0, with bit 31 set when
@@ -128,12 +141,13 @@ struct ElemArgs {
 // one job of a batched packed gather (emg_gather_batch)
 struct GatherJob {
   const int32_t *ent_ptr, *order;
-  const void *pidx;
-  const uint16_t *posoff;
+  const void *pidx;       // packed: int2 records; block: uint32 block records
+  const uint16_t *posoff; // packed: list start per position; block: per row pair
   const int32_t *indptr;
+  const uint32_t *ent_cnt;  // block layout: adjacent edges | faces << 16 per entity
   const void *values;
   double2 *A;
-  int64_t E, F, n_values, n_ctas;
+  int64_t E, F, n_values, n_ctas;  // n_values: value slots (packed) or blocks (block layout)
 };
 
 // Gather chunks: a warp owns CHUNK consecutive entities of one kind. Their
@@ -180,7 +194,7 @@ EMG_DECLARE_ELEM(2, 2)
 
 #define EMG_DECLARE_ELEM_BATCH(F, K)                                                                      \
   int launch_element_batch_##F##_##K(const ElemArgs *d_jobs, const int64_t *d_cta_start, int n_jobs, \
-                                     int64_t total_ctas, cudaStream_t s);
+                                     int64_t total_ctas, int layout, cudaStream_t s);
 EMG_DECLARE_ELEM_BATCH(0, 0)
 EMG_DECLARE_ELEM_BATCH(0, 1)
 EMG_DECLARE_ELEM_BATCH(0, 2)
@@ -224,7 +238,7 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *indptr, 
 int gather_job_fill(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_values, void *d_A,
                     GatherJob *out);
 int launch_gather_batch(const GatherJob *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total_ctas,
-                        int precision, cudaStream_t s);
+                        int precision, int layout, cudaStream_t s);
 int launch_form_sweep(const void *K, const void *M, const void *P, int64_t nnz, const double *coef, int nf,
                       void *out, int64_t stride, cudaStream_t s);
 int launch_form_batch(const emg_form_item *items, const int64_t *tile_start, const int32_t *n_items, int max_items,

@@ -569,7 +569,7 @@ __device__ __forceinline__ void do_row(const Tensors<KIND, R> &T, const R *mu, d
   const int lane = threadIdx.x & 31;
   const int rx = ref_dof(inv, X);
   if (active)
-    compute_row<X, FORM, KIND, R>(T, mu, sig, cK, cM, inv, rx, stage + lane * 20,
+    compute_row<X, FORM, KIND, R>(T, mu, sig, cK, cM, inv, rx, stage + lane * 21,
                                   std::make_integer_sequence<int, 20>{});
   __syncwarp();
   // cooperative, coalesced write of the warp's 32 rows (each 20 contiguous values)
@@ -580,7 +580,7 @@ __device__ __forceinline__ void do_row(const Tensors<KIND, R> &T, const R *mu, d
     int ia_r = __shfl_sync(0xffffffffu, ia, r);
     int a_r = __shfl_sync(0xffffffffu, rx, r);
     bool act_r = __shfl_sync(0xffffffffu, (int)active, r);
-    if (act_r) out[(int64_t)ia_r * 400 + a_r * 20 + c] = stage[r * 20 + c];
+    if (act_r) out[(int64_t)ia_r * 400 + a_r * 20 + c] = stage[r * 21 + c];
   }
   __syncwarp();
 }
@@ -640,7 +640,7 @@ __device__ __forceinline__ void do_row_packed(const Tensors<KIND, R> &T, const R
   constexpr int W = 20 - X;
   const int lane = threadIdx.x & 31;
   if (active)
-    compute_row_packed<X, FORM, KIND, R>(T, mu, sig, cK, cM, inv, stage + lane * W,
+    compute_row_packed<X, FORM, KIND, R>(T, mu, sig, cK, cM, inv, stage + lane * (W | 1),
                                          std::make_integer_sequence<int, W>{});
   __syncwarp();
 #pragma unroll 1
@@ -649,7 +649,7 @@ __device__ __forceinline__ void do_row_packed(const Tensors<KIND, R> &T, const R
     const int r = e / W, c = e - r * W;
     const int ia_r = __shfl_sync(0xffffffffu, ia, r);
     const bool act_r = __shfl_sync(0xffffffffu, (int)active, r);
-    if (act_r) out[(int64_t)ia_r * 210 + packed_index(X, X) + c] = stage[r * W + c];
+    if (act_r) out[(int64_t)ia_r * 210 + packed_index(X, X) + c] = stage[r * (W | 1) + c];
   }
   __syncwarp();
 }
@@ -662,17 +662,73 @@ __device__ __forceinline__ void all_rows_packed(const Tensors<KIND, R> &T, const
   (do_row_packed<FORM, KIND, R, Xs>(T, mu, sig, cK, cM, inv, active, ia, stage, out), ...);
 }
 
+// ---- entity-pair block layout: value[ia*220 + 4*block_index(i, j) + k] for
+// canonical entities i <= j. Block row i (its 10 - i blocks, 4 values each)
+// is staged in shared memory and the warp writes its 32 block rows as
+// contiguous runs. Each value is the packed layout's (min, max) entry.
+template <int x, int y, int FORM, int KIND, typename R>
+__device__ __forceinline__ void compute_store_any(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                                  const CR<R> &cM, uint64_t inv, typename StoreT<R>::T *dst) {
+  constexpr int lo = x < y ? x : y, hi = x < y ? y : x;
+  compute_store_packed<lo, hi, FORM, KIND, R>(T, mu, sig, cK, cM, inv, dst - (hi - lo));
+}
+
+template <int i, int FORM, int KIND, typename R, int... Js>
+__device__ __forceinline__ void compute_block_row(const Tensors<KIND, R> &T, const R *mu, double sig,
+                                                  const CR<R> &cK, const CR<R> &cM, uint64_t inv,
+                                                  typename StoreT<R>::T *row, std::integer_sequence<int, Js...>) {
+  // the first DoF's entries of the block row, then the second's (row order of the packed triangle)
+  ((compute_store_any<ent_dof1(i), ent_dof1(i + Js), FORM, KIND, R>(T, mu, sig, cK, cM, inv, row + 4 * Js + 0),
+    compute_store_any<ent_dof1(i), ent_dof2(i + Js), FORM, KIND, R>(T, mu, sig, cK, cM, inv, row + 4 * Js + 1)),
+   ...);
+  ((compute_store_any<ent_dof2(i), ent_dof1(i + Js), FORM, KIND, R>(T, mu, sig, cK, cM, inv, row + 4 * Js + 2),
+    compute_store_any<ent_dof2(i), ent_dof2(i + Js), FORM, KIND, R>(T, mu, sig, cK, cM, inv, row + 4 * Js + 3)),
+   ...);
+}
+
+template <int FORM, int KIND, typename R, int I>
+__device__ __forceinline__ void do_row_block(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                             const CR<R> &cM, uint64_t inv, bool active, int ia,
+                                             typename StoreT<R>::T *stage, typename StoreT<R>::T *out) {
+  constexpr int W = 4 * (10 - I);
+  const int lane = threadIdx.x & 31;
+  if (active)
+    compute_block_row<I, FORM, KIND, R>(T, mu, sig, cK, cM, inv, stage + lane * (W | 1),
+                                        std::make_integer_sequence<int, 10 - I>{});
+  __syncwarp();
+#pragma unroll 1
+  for (int it = 0; it < W; ++it) {
+    const int e = it * 32 + lane;
+    const int r = e / W, c = e - r * W;
+    const int ia_r = __shfl_sync(0xffffffffu, ia, r);
+    const bool act_r = __shfl_sync(0xffffffffu, (int)active, r);
+    if (act_r) out[(int64_t)ia_r * kBlockValues + 4 * block_index(I, I) + c] = stage[r * (W | 1) + c];
+  }
+  __syncwarp();
+}
+
+template <int FORM, int KIND, typename R, int... Is>
+__device__ __forceinline__ void all_rows_block(const Tensors<KIND, R> &T, const R *mu, double sig, const CR<R> &cK,
+                                               const CR<R> &cM, uint64_t inv, bool active, int ia,
+                                               typename StoreT<R>::T *stage, typename StoreT<R>::T *out,
+                                               std::integer_sequence<int, Is...>) {
+  (do_row_block<FORM, KIND, R, Is>(T, mu, sig, cK, cM, inv, active, ia, stage, out), ...);
+}
+
 // LAYOUT 0: the reference's COO block [ia][a][b] (400 values, each entry
 //           computed in both of its rows);
-// LAYOUT 1: the packed canonical upper triangle [ia][210] (the assembly
-//           path, each unique entry computed once)
+// LAYOUT 1: the packed canonical upper triangle [ia][210] (each unique
+//           entry computed once);
+// LAYOUT 2: the entity-pair blocks [ia][220] (the assembly path)
 // One CTA's 128 tets, assembled indices ia0 .. ia0 + 127 of the job a (every
 // thread of the CTA calls it with the same ia0).
 template <int FORM, int KIND, int LAYOUT>
 __device__ __forceinline__ void element_cta(const ElemArgs &a, int64_t ia0, unsigned char *stage_raw) {
   using R = typename FormReal<FORM>::T;
   using ST = typename StoreT<R>::T;
-  constexpr int STAGE = 20;  // values per lane
+  // values per lane: a row's stride is odd (in values), so the 32 lanes'
+  // stores of one value position fall in distinct shared-memory bank groups
+  constexpr int STAGE = LAYOUT == 2 ? 41 : 21;
   ST *stage = reinterpret_cast<ST *>(stage_raw) + (threadIdx.x >> 5) * (32 * STAGE);
   ST *out = reinterpret_cast<ST *>(a.out);
   const int64_t ia64 = ia0 + threadIdx.x;
@@ -746,6 +802,9 @@ __device__ __forceinline__ void element_cta(const ElemArgs &a, int64_t ia0, unsi
   }
   if constexpr (LAYOUT == 0) {
     all_rows<FORM, KIND, R>(T, mu, sig, cK, cM, inv, active, ia, stage, out, std::make_integer_sequence<int, 20>{});
+  } else if constexpr (LAYOUT == 2) {
+    all_rows_block<FORM, KIND, R>(T, mu, sig, cK, cM, inv, active, ia, stage, out,
+                                  std::make_integer_sequence<int, 10>{});
   } else {
     all_rows_packed<FORM, KIND, R>(T, mu, sig, cK, cM, inv, active, ia, stage, out,
                                    std::make_integer_sequence<int, 20>{});
@@ -761,7 +820,7 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
 // Several jobs (meshes, materials, coefficients, outputs) in one launch of
 // the packed form: job j owns the CTAs [cta_start[j], cta_start[j + 1]) and
 // its tets in CTA order, as if launched alone.
-template <int FORM, int KIND>
+template <int FORM, int KIND, int LAYOUT>
 __global__ void __launch_bounds__(ELEM_THREADS) k_element_batch(const ElemArgs *jobs, const int64_t *cta_start,
                                                                 int n_jobs) {
   extern __shared__ __align__(16) unsigned char stage_raw[];
@@ -773,13 +832,13 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element_batch(const ElemArgs *
     else hi = mid - 1;
   }
   if (n_jobs <= 0 || b >= cta_start[n_jobs]) return;
-  element_cta<FORM, KIND, 1>(jobs[lo], (b - cta_start[lo]) * ELEM_THREADS, stage_raw);
+  element_cta<FORM, KIND, LAYOUT>(jobs[lo], (b - cta_start[lo]) * ELEM_THREADS, stage_raw);
 }
 
 template <int FORM, int KIND, int LAYOUT>
 int launch_element_t(const ElemArgs &a, cudaStream_t s) {
   using ST = typename StoreT<typename FormReal<FORM>::T>::T;
-  constexpr size_t smem = (size_t)ELEM_WARPS * 32 * 20 * sizeof(ST);
+  constexpr size_t smem = (size_t)ELEM_WARPS * 32 * (LAYOUT == 2 ? 41 : 21) * sizeof(ST);
   // the attribute belongs to the current device: set once per device (benign
   // race: every thread that gets here sets the same value)
   static bool configured[64] = {false};
@@ -796,23 +855,25 @@ int launch_element_t(const ElemArgs &a, cudaStream_t s) {
   return launch_check("k_element");
 }
 
-template <int FORM, int KIND>
+template <int FORM, int KIND, int LAYOUT>
 int launch_element_batch_t(const ElemArgs *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total_ctas,
                            cudaStream_t s) {
   using ST = typename StoreT<typename FormReal<FORM>::T>::T;
-  constexpr size_t smem = (size_t)ELEM_WARPS * 32 * 20 * sizeof(ST);
+  constexpr size_t smem = (size_t)ELEM_WARPS * 32 * (LAYOUT == 2 ? 41 : 21) * sizeof(ST);  // element_cta's stage
   static bool configured[64] = {false};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
   if (dev >= 64 || !configured[dev]) {
     cudaError_t e =
-        cudaFuncSetAttribute(k_element_batch<FORM, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_element_batch<FORM, KIND, LAYOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
     if (e != cudaSuccess) return fail(EMG_ECUDA, "cudaFuncSetAttribute(k_element_batch): %s", cudaGetErrorString(e));
     if (dev < 64) configured[dev] = true;
   }
   if (n_jobs == 0 || total_ctas == 0) return EMG_OK;
   if (total_ctas > INT32_MAX) return fail(EMG_ERANGE, "too many CTAs (%lld)", (long long)total_ctas);
-  k_element_batch<FORM, KIND><<<(unsigned)total_ctas, ELEM_THREADS, smem, s>>>(d_jobs, d_cta_start, n_jobs);
+  k_element_batch<FORM, KIND, LAYOUT><<<(unsigned)total_ctas, ELEM_THREADS, smem, s>>>(d_jobs, d_cta_start,
+                                                                                       n_jobs);
   return launch_check("k_element_batch");
 }
 
@@ -820,6 +881,7 @@ template <int FORM, int KIND>
 int launch_element_k(const ElemArgs &a, int layout, cudaStream_t s) {
   if (layout == EMG_LAYOUT_COO) return launch_element_t<FORM, KIND, 0>(a, s);
   if (layout == EMG_LAYOUT_PACKED) return launch_element_t<FORM, KIND, 1>(a, s);
+  if (layout == EMG_LAYOUT_BLOCK) return launch_element_t<FORM, KIND, 2>(a, s);
   return fail(EMG_EINVAL, "bad layout %d", layout);
 }
 

@@ -48,6 +48,8 @@ __device__ __forceinline__ void load_coo_pair(const void *v, int ia, int slot, i
 struct ChunkMeta {
   int32_t I0, I1, A0, A1, Lsum;
   int64_t hbase;
+  int64_t x0, cb0;  // first entity of the chunk and its first-DoF column
+  int nx;           // entities in the chunk
 };
 
 // Processing position g -> chunk through the plan's order array (the default
@@ -81,6 +83,9 @@ __device__ __forceinline__ bool chunk_meta(const int32_t *ent_ptr, const int32_t
   m.A1 = __shfl_sync(0xffffffffu, meta, 4);
   const int32_t cE = __shfl_sync(0xffffffffu, meta, 5), c2E = __shfl_sync(0xffffffffu, meta, 6);
   m.hbase = edges ? (int64_t)m.A0 : (int64_t)cE + (m.A0 - c2E);
+  m.x0 = x0;
+  m.cb0 = cb0;
+  m.nx = nx;
   return true;
 }
 
@@ -216,6 +221,94 @@ __global__ void __launch_bounds__(PackedShape<R, COMPACT>::warps * 32, PackedSha
   gather_packed_chunk<R, COMPACT>(m, pidx_v, posoff, n_values, v, ar, ai, A, slot2);
 }
 
+// ---- entity-pair block layout (EMG_LAYOUT_BLOCK). A lane owns a row pair of
+// the chunk's first-DoF runs -- the first-DoF row p of an adjacent entity and
+// its partner row p' (the entity's second DoF) -- and sums, over the tets of
+// its list in item order, the 2x2 blocks of that entity pair: the entries of
+// rows p, p' in the chunk entity's two columns. One 4-byte record and one
+// contiguous 64-byte (32-byte) read give four entries of A; every entry sums
+// the same values in the same order as the packed gather.
+constexpr int BG_WARPS = 4;
+
+template <typename R>
+__device__ __forceinline__ void gather_block_chunk(const ChunkMeta &m, const uint32_t *brec, const uint16_t *hoff,
+                                                   const int32_t *indptr, const uint32_t *ent_cnt, int64_t n_blocks,
+                                                   const void *v, double ar, double ai, double2 *A,
+                                                   int32_t *se /* 3 * CHUNK + 1 ints of this warp */) {
+  const int lane = threadIdx.x & 31;
+  int32_t *hs = se;                  // half start of entity e in the chunk, hs[nx] = all row pairs
+  int32_t *nes = se + CHUNK + 1;     // adjacent edges of entity e
+  int32_t *cs = se + 2 * CHUNK + 1;  // first-DoF column start of entity e, relative to A0
+  if (lane < m.nx) {
+    const int32_t c = indptr[m.cb0 + lane] - m.A0;
+    cs[lane] = c;
+    hs[lane] = c / 2;
+    nes[lane] = (int32_t)(ent_cnt[m.x0 + lane] & 0xffffu);
+  }
+  if (lane == 0) hs[m.nx] = m.Lsum / 2;
+  __syncwarp();
+  const int H = m.Lsum / 2;
+  const int total = 10 * (m.I1 - m.I0);
+  const uint32_t *rl = brec + (int64_t)10 * m.I0;
+  const int64_t hb = m.hbase / 2;
+  int e = 0;
+  // list bounds of the lane's next row pair are loaded while the current one is summed
+  int n0 = 0, n1 = 0;
+  if (lane < H) {
+    n0 = hoff[hb + lane];
+    n1 = lane + 1 < H ? (int)hoff[hb + lane + 1] : total;
+  }
+  for (int h = lane; h < H; h += 32) {
+    while (e + 1 < m.nx && h >= hs[e + 1]) ++e;  // h only grows along a lane
+    const int hl = h - hs[e], ne = nes[e];
+    const int nf = hs[e + 1] - hs[e] - ne;
+    const int p = hl < ne ? cs[e] + hl : cs[e] + ne + hl;
+    const int pp = hl < ne ? p + ne : p + nf;
+    const int o0 = n0;
+    const int o1 = min(n1, total);
+    if (h + 32 < H) {
+      n0 = hoff[hb + h + 32];
+      n1 = h + 33 < H ? (int)hoff[hb + h + 33] : total;
+    }
+    double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0, s2r = 0.0, s2i = 0.0, s3r = 0.0, s3i = 0.0;
+    for (int k = o0; k < o1; ++k) {
+      const uint32_t rec = __ldg(rl + k);
+      const int64_t b = rec & 0x7fffffffu;
+      if (b >= n_blocks) continue;  // only a plan whose build was flagged can hold this
+      const C64 u0 = load_val<R>(v, 4 * b), u3 = load_val<R>(v, 4 * b + 3);
+      C64 u1 = load_val<R>(v, 4 * b + 1), u2 = load_val<R>(v, 4 * b + 2);
+      if (rec >> 31) {
+        const C64 t = u1;
+        u1 = u2;
+        u2 = t;
+      }
+      s0r += u0.re;
+      s0i += u0.im;
+      s1r += u1.re;
+      s1i += u1.im;
+      s2r += u2.re;
+      s2i += u2.im;
+      s3r += u3.re;
+      s3i += u3.im;
+    }
+    A[m.A0 + p] = make_double2(ar * s0r - ai * s0i, ar * s0i + ai * s0r);
+    A[m.A1 + p] = make_double2(ar * s1r - ai * s1i, ar * s1i + ai * s1r);
+    A[m.A0 + pp] = make_double2(ar * s2r - ai * s2i, ar * s2i + ai * s2r);
+    A[m.A1 + pp] = make_double2(ar * s3r - ai * s3i, ar * s3i + ai * s3r);
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(BG_WARPS * 32, 10)
+    k_gather_block(const int32_t *ent_ptr, const int32_t *order, const uint32_t *brec, const uint16_t *hoff,
+                   const uint32_t *ent_cnt, int64_t E, int64_t F, int64_t n_blocks, const int32_t *indptr,
+                   const void *v, double ar, double ai, double2 *A) {
+  __shared__ int32_t se[BG_WARPS][3 * CHUNK + 1];
+  ChunkMeta m;
+  if (!chunk_meta(ent_ptr, order, indptr, E, F, (int64_t)blockIdx.x * BG_WARPS + (threadIdx.x >> 5), m)) return;
+  gather_block_chunk<R>(m, brec, hoff, indptr, ent_cnt, n_blocks, v, ar, ai, A, se[threadIdx.x >> 5]);
+}
+
 // Several jobs' packed gathers (8-byte records, alpha = 1) in one launch: job
 // j owns the CTAs [cta_start[j], cta_start[j + 1]) and its chunks in CTA
 // order, as if launched alone.
@@ -236,6 +329,27 @@ __global__ void __launch_bounds__(PackedShape<R, false>::warps * 32, PackedShape
                   (b - cta_start[lo]) * PackedShape<R, false>::warps + (threadIdx.x >> 5), m))
     return;
   gather_packed_chunk<R, false>(m, j.pidx, j.posoff, j.n_values, j.values, 1.0, 0.0, j.A, nullptr);
+}
+
+// Several jobs' block gathers (alpha = 1) in one launch, as k_gather_packed_batch.
+template <typename R>
+__global__ void __launch_bounds__(BG_WARPS * 32, 10)
+    k_gather_block_batch(const GatherJob *jobs, const int64_t *cta_start, int n_jobs) {
+  __shared__ int32_t se[BG_WARPS][3 * CHUNK + 1];
+  const int64_t b = blockIdx.x;
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cta_start[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  if (n_jobs <= 0 || b >= cta_start[n_jobs]) return;
+  const GatherJob &j = jobs[lo];
+  ChunkMeta m;
+  if (!chunk_meta(j.ent_ptr, j.order, j.indptr, j.E, j.F, (b - cta_start[lo]) * BG_WARPS + (threadIdx.x >> 5), m))
+    return;
+  gather_block_chunk<R>(m, static_cast<const uint32_t *>(j.pidx), j.posoff, j.indptr, j.ent_cnt, j.n_values,
+                        j.values, 1.0, 0.0, j.A, se[threadIdx.x >> 5]);
 }
 
 // ---------------------------------------------------------------------------
@@ -331,7 +445,8 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
   (void)d_status;
   if (p->n_ent == 0) return EMG_OK;
   if (precision < EMG_FP64 || precision > EMG_EXACT) return fail(EMG_EINVAL, "bad precision %d", precision);
-  if (layout != EMG_LAYOUT_COO && layout != EMG_LAYOUT_PACKED) return fail(EMG_EINVAL, "bad layout %d", layout);
+  if (layout != EMG_LAYOUT_COO && layout != EMG_LAYOUT_PACKED && layout != EMG_LAYOUT_BLOCK)
+    return fail(EMG_EINVAL, "bad layout %d", layout);
   const char *plan = static_cast<const char *>(d_plan);
   const int32_t *ent_ptr = reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr);
   const Item *items = reinterpret_cast<const Item *>(plan + p->off_item);
@@ -342,6 +457,21 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
   double2 *A = static_cast<double2 *>(d_A);
   const bool two = d_v2 != nullptr;
   const bool f32 = values_fp32(precision);
+  if (layout == EMG_LAYOUT_BLOCK) {
+    if (two) return fail(EMG_EINVAL, "the block layout takes one value array");
+    const uint32_t *brec = reinterpret_cast<const uint32_t *>(plan + p->off_pidx);
+    const uint16_t *hoff = reinterpret_cast<const uint16_t *>(plan + p->off_hoff);
+    const uint32_t *ent_cnt = reinterpret_cast<const uint32_t *>(plan + p->off_ent_cnt);
+    const int gb = grid_for(n_chunks(p->n_edges, p->n_tris), BG_WARPS);
+    const int64_t nb = p->n_assy * 55;
+    if (f32)
+      k_gather_block<float><<<gb, BG_WARPS * 32, 0, s>>>(ent_ptr, order, brec, hoff, ent_cnt, p->n_edges, p->n_tris,
+                                                          nb, d_indptr, d_v1, ar, ai, A);
+    else
+      k_gather_block<double><<<gb, BG_WARPS * 32, 0, s>>>(ent_ptr, order, brec, hoff, ent_cnt, p->n_edges,
+                                                           p->n_tris, nb, d_indptr, d_v1, ar, ai, A);
+    return launch_check("k_gather_block");
+  }
   if (layout == EMG_LAYOUT_PACKED) {
     if (two) return fail(EMG_EINVAL, "the packed layout takes one value array");
     const void *pidx = plan + p->off_pidx;
@@ -373,27 +503,37 @@ int launch_gather(const emg_plan *p, const void *d_plan, const int32_t *d_indptr
 
 int gather_job_fill(const emg_plan *p, const void *d_plan, const int32_t *d_indptr, const void *d_values, void *d_A,
                     GatherJob *out) {
-  if (p->record_bytes != 8) return fail(EMG_EINVAL, "batched gathers take plans with 8-byte records");
+  const bool block = p->value_layout == EMG_LAYOUT_BLOCK;
+  if (!block && p->record_bytes != 8)
+    return fail(EMG_EINVAL, "batched gathers take block-layout plans or packed ones with 8-byte records");
   const char *plan = static_cast<const char *>(d_plan);
   out->ent_ptr = reinterpret_cast<const int32_t *>(plan + p->off_ent_ptr);
   out->order = reinterpret_cast<const int32_t *>(plan + p->off_order);
   out->pidx = plan + p->off_pidx;
-  out->posoff = reinterpret_cast<const uint16_t *>(plan + p->off_posoff);
+  out->posoff = reinterpret_cast<const uint16_t *>(plan + (block ? p->off_hoff : p->off_posoff));
   out->indptr = d_indptr;
+  out->ent_cnt = reinterpret_cast<const uint32_t *>(plan + p->off_ent_cnt);
   out->values = d_values;
   out->A = static_cast<double2 *>(d_A);
   out->E = p->n_edges;
   out->F = p->n_tris;
-  out->n_values = p->n_assy * 210;
-  out->n_ctas = (n_chunks(p->n_edges, p->n_tris) + PackedShape<double, false>::warps - 1) /
-                PackedShape<double, false>::warps;
+  out->n_values = p->n_assy * (block ? 55 : 210);
+  const int warps = block ? BG_WARPS : PackedShape<double, false>::warps;
+  out->n_ctas = (n_chunks(p->n_edges, p->n_tris) + warps - 1) / warps;
   return EMG_OK;
 }
 
 int launch_gather_batch(const GatherJob *d_jobs, const int64_t *d_cta_start, int n_jobs, int64_t total_ctas,
-                        int precision, cudaStream_t s) {
+                        int precision, int layout, cudaStream_t s) {
   if (n_jobs == 0 || total_ctas == 0) return EMG_OK;
   if (total_ctas > INT32_MAX) return fail(EMG_ERANGE, "too many CTAs (%lld)", (long long)total_ctas);
+  if (layout == EMG_LAYOUT_BLOCK) {
+    if (values_fp32(precision))
+      k_gather_block_batch<float><<<(unsigned)total_ctas, BG_WARPS * 32, 0, s>>>(d_jobs, d_cta_start, n_jobs);
+    else
+      k_gather_block_batch<double><<<(unsigned)total_ctas, BG_WARPS * 32, 0, s>>>(d_jobs, d_cta_start, n_jobs);
+    return launch_check("k_gather_block_batch");
+  }
   static_assert(PackedShape<double, false>::warps == PackedShape<float, false>::warps, "same chunks per CTA");
   if (values_fp32(precision))
     k_gather_packed_batch<float><<<(unsigned)total_ctas, PackedShape<float, false>::warps * 32, 0, s>>>(

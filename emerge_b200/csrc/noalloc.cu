@@ -11,8 +11,9 @@ namespace emg {
 namespace {
 
 // 96 MiB of element-value scratch, held by every GPU that loads the library
-// until the process exits: 29,959 assembled tets in FP64/exact form (3360 B
-// of packed element values per tet), 59,918 in the mixed form (1680 B).
+// until the process exits: 28,597 assembled tets in FP64/exact form (3520 B
+// of element values per tet, the workspace size of either value layout),
+// 57,195 in the mixed form (1760 B).
 constexpr size_t kStaticValuesBytes = size_t(96) << 20;
 static __device__ __align__(256) unsigned char g_static_values[kStaticValuesBytes];
 

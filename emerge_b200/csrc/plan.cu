@@ -384,13 +384,93 @@ __global__ void __launch_bounds__(CC_WARPS * 32)
           const int al = canon_dof(rec.ranks, r);
           const int b0 = canon_dof(rec.ranks, a0), b1 = canon_dof(rec.ranks, a1);
           const int64_t base = (int64_t)rec.ia * 210;
-          if (compact)
+          if (pidx_v && compact)
             static_cast<uint32_t *>(pidx_v)[(int64_t)20 * I0 + at] =
                 (uint32_t)(base + packed_index(min(al, b0), max(al, b0))) | (al <= b0 ? 0x80000000u : 0u);
-          else
+          else if (pidx_v)
             static_cast<int2 *>(pidx_v)[(int64_t)20 * I0 + at] =
                 make_int2((int)(base + packed_index(min(al, b0), max(al, b0))),
                           (int)(base + packed_index(min(al, b1), max(al, b1))));
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Block gather lists (EMG_LAYOUT_BLOCK), warp per chunk: every (item, row
+// entity) of the chunk contributes the tet's block of that entity pair to one
+// row pair (the row entity's first-DoF row and its partner row, which hold the
+// same tets); counted per row pair, scanned into hoff (list start relative to
+// the chunk's first record, 10 * I0), then placed in item order, so each
+// output sums its contributions in the order of the packed lists.
+__global__ void __launch_bounds__(CC_WARPS * 32)
+    k_chunk_blocks(const int32_t *ent_ptr, const Item *items, const uint32_t *ent_cnt, int64_t E, int64_t F,
+                   const int32_t *indptr, uint16_t *hoff, uint32_t *brec, int64_t *st) {
+  __shared__ int32_t cnt_all[CC_WARPS][CHUNK_MAX_POS / 2];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t chunk = (int64_t)blockIdx.x * CC_WARPS + w;
+  const int64_t nec = n_edge_chunks(E);
+  if (chunk >= n_chunks(E, F)) return;
+  const bool edges = chunk < nec;
+  const int64_t x0 = edges ? chunk * CHUNK : E + (chunk - nec) * CHUNK;
+  const int nx = (int)min((int64_t)CHUNK, (edges ? E : E + F) - x0);
+  const int64_t cb0 = edges ? x0 : E + x0;
+  const int32_t my_ptr = lane <= nx ? ent_ptr[x0 + lane] : 0;
+  const int32_t my_c0 = lane <= nx ? indptr[cb0 + lane] : 0;
+  const uint32_t my_cnt = lane < nx ? ent_cnt[x0 + lane] : 0u;
+  const int32_t I0 = __shfl_sync(0xffffffffu, my_ptr, 0), I1 = __shfl_sync(0xffffffffu, my_ptr, nx);
+  const int32_t A0 = __shfl_sync(0xffffffffu, my_c0, 0), A0e = __shfl_sync(0xffffffffu, my_c0, nx);
+  const int Lsum = A0e - A0, Hsum = Lsum / 2;
+  if (Lsum > CHUNK_MAX_POS || I1 - I0 > CHUNK_MAX_ITEMS) {
+    if (lane == 0) flag(st, EMG_ST_CAPACITY, x0);
+    return;
+  }
+  const int64_t hb = (edges ? (int64_t)A0 : (int64_t)indptr[E] + (A0 - indptr[2 * E])) / 2;
+  int32_t *cnt = cnt_all[w];
+  for (int i = lane; i < Hsum; i += 32) cnt[i] = 0;
+  const int r = lane;  // row entity slot (0-5 edges, 6-9 faces) of the item's tet
+  __syncwarp();
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      int32_t carry = 0;
+      for (int b0 = 0; b0 < Hsum; b0 += 32) {
+        const int i = b0 + lane;
+        const int32_t v = i < Hsum ? cnt[i] : 0;
+        int32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        if (i < Hsum) {
+          cnt[i] = carry + x - v;
+          hoff[hb + i] = (uint16_t)(carry + x - v);
+        }
+        carry += __shfl_sync(0xffffffffu, x, 31);
+      }
+      __syncwarp();
+    }
+    for (int32_t k = I0; k < I1; ++k) {
+      if (r < 10) {
+        int e = 0;
+        for (int q = 1; q < nx; ++q)
+          if (k >= __shfl_sync(0x3ffu, my_ptr, q)) e = q;
+        const int32_t ce = __shfl_sync(0x3ffu, my_c0, e);
+        const uint32_t c = __shfl_sync(0x3ffu, my_cnt, e);
+        const int ne = (int)(c & 0xffffu);
+        const Item rec = items[k];
+        const int h = (ce - A0) / 2 + (r < 6 ? 0 : ne) + rec.pos[r];
+        if (pass == 0) {
+          cnt[h] += 1;  // distinct h across the 10 lanes of one item
+        } else {
+          const int32_t at = cnt[h]++;
+          const int s = rec.slot;
+          const int cb = s < 6 ? canon_dof(rec.ranks, s) : canon_dof(rec.ranks, 12 + (s - 6)) - 6;
+          const int ca = r < 6 ? canon_dof(rec.ranks, r) : canon_dof(rec.ranks, 12 + (r - 6)) - 6;
+          const int lo = ca < cb ? ca : cb, hi = ca < cb ? cb : ca;
+          brec[(int64_t)10 * I0 + at] =
+              (uint32_t)((int64_t)rec.ia * 55 + block_index(lo, hi)) | (ca > cb ? 0x80000000u : 0u);
         }
       }
       __syncwarp();
@@ -537,9 +617,14 @@ size_t plan_layout(emg_plan *p) {
   p->off_posoff = o;
   o = align_up(o + (size_t)p->n_items * 20 * 2, 256);
   // per contribution the packed-layout indices of its two values (first- and
-  // second-DoF column), in the same order as contrib
+  // second-DoF column), in the same order as contrib; block layout: one
+  // 4-byte block record per (item, row entity) and a uint16 list start per
+  // row pair (at most 10 per item)
+  const bool block = p->value_layout == EMG_LAYOUT_BLOCK;
   p->off_pidx = o;
-  o = align_up(o + (size_t)p->n_items * 20 * (p->record_bytes == 4 ? 4 : 8), 256);
+  o = align_up(o + (size_t)p->n_items * (block ? 10 * 4 : 20 * (p->record_bytes == 4 ? 4 : 8)), 256);
+  p->off_hoff = o;
+  o = align_up(o + (block ? (size_t)p->n_items * 10 * 2 : 0), 256);
   // the gather's chunk processing order
   p->off_order = o;
   o = align_up(o + (size_t)n_chunks(p->n_edges, p->n_tris) * 4, 256);
@@ -647,9 +732,18 @@ int plan_finish(const emg_plan *p, const int32_t *d_t2e, const int32_t *d_t2t, c
   uint16_t *posoff = reinterpret_cast<uint16_t *>(plan + p->off_posoff);
   void *pidx = plan + p->off_pidx;
   const bool compact = p->record_bytes == 4;
+  const bool block = p->value_layout == EMG_LAYOUT_BLOCK;
+  // the block layout keeps the (item, row) lists for the COO gather and puts
+  // its own records where the packed records would be
   k_chunk_contrib<<<grid_for(n_chunks(p->n_edges, p->n_tris), CC_WARPS), CC_WARPS * 32, 0, s>>>(
-      ent_ptr, items, ent_cnt, p->n_edges, p->n_tris, d_indptr, contrib, posoff, pidx, compact, d_status);
-  return launch_check("k_chunk_contrib");
+      ent_ptr, items, ent_cnt, p->n_edges, p->n_tris, d_indptr, contrib, posoff, block ? nullptr : pidx, compact,
+      d_status);
+  if ((rc = launch_check("k_chunk_contrib"))) return rc;
+  if (!block) return EMG_OK;
+  k_chunk_blocks<<<grid_for(n_chunks(p->n_edges, p->n_tris), CC_WARPS), CC_WARPS * 32, 0, s>>>(
+      ent_ptr, items, ent_cnt, p->n_edges, p->n_tris, d_indptr, reinterpret_cast<uint16_t *>(plan + p->off_hoff),
+      static_cast<uint32_t *>(pidx), d_status);
+  return launch_check("k_chunk_blocks");
 }
 
 int sort_u64(uint64_t *keys, int64_t n2, cudaStream_t s) {

@@ -107,19 +107,22 @@ def floor_bytes(n_nodes: int, n_tets: int, nnz: int, material_bytes_per_tet: int
     return 24 * n_nodes + 16 * n_tets + material_bytes_per_tet * n_tets + 16 * nnz
 
 
-def element_alg_bytes(n_nodes: int, n_tets: int, value_bytes: int, material_bytes_per_tet: int = 16) -> int:
+def element_alg_bytes(n_nodes: int, n_tets: int, value_bytes: int, material_bytes_per_tet: int = 16,
+                      values_per_tet: int = 220) -> int:
     """Algorithmic bytes of one element-kernel launch: nodes + tets + material
-    read, 210 packed block values per tet written (value_bytes = 16 for
+    read, the element values written (values_per_tet = 220 in the entity-pair
+    block layout, 210 in the packed triangle; value_bytes = 16 for
     complex128, 8 for complex64)."""
-    return 24 * n_nodes + 16 * n_tets + material_bytes_per_tet * n_tets + 210 * value_bytes * n_tets
+    return (24 * n_nodes + 16 * n_tets + material_bytes_per_tet * n_tets
+            + values_per_tet * value_bytes * n_tets)
 
 
-def gather_alg_bytes(n_tets: int, nnz: int, value_bytes: int) -> int:
-    """Algorithmic bytes of one gather launch: the packed values read once,
+def gather_alg_bytes(n_tets: int, nnz: int, value_bytes: int, values_per_tet: int = 220) -> int:
+    """Algorithmic bytes of one gather launch: the element values read once,
     the int32 slot->nnz map (4 B per COO slot) and segment offsets, complex128
     A written. element_alg_bytes + gather_alg_bytes = alg_bytes + the
-    2 x 210 x value_bytes per tet of the intermediate round trip."""
-    return 210 * value_bytes * n_tets + 4 * 400 * n_tets + 4 * (nnz + 1) + 16 * nnz
+    2 x values_per_tet x value_bytes per tet of the intermediate round trip."""
+    return values_per_tet * value_bytes * n_tets + 4 * 400 * n_tets + 4 * (nnz + 1) + 16 * nnz
 
 
 def wr90_pml_slivers(n=(84, 50, 40), jitter=0.05, seed=4, freq=10e9, shell=0.10, sliver_frac=0.02,

@@ -94,6 +94,14 @@ enum {
   EMG_LAYOUT_COO_T = 2,  /* D x D blocks per tet, transposed: value (i, j) of tet t
                             at D^2 t + D j + i (the Lagrange-2 element values
                             read by the COO gather with block_dofs = D) */
+  EMG_LAYOUT_BLOCK = 3,  /* entity-pair blocks in the canonical frame: for the
+                            tet's 10 entities (0-5 edges, 6-9 faces) and each
+                            pair i <= j, the 2x2 values of their first and
+                            second DoFs [(i1,j1), (i1,j2), (i2,j1), (i2,j2)]
+                            at value[ia*220 + 4*(i*(21-i)/2 + j-i) + k]
+                            (i1 = i, i2 = i+6 for edges; 12+i-6, 16+i-6 for
+                            faces): one gather record and one 64-byte read
+                            (32 for complex64) serve four entries of A */
 };
 
 typedef struct {
@@ -122,6 +130,9 @@ typedef struct {
   size_t plan_bytes;      /* blob size */
   size_t workspace_bytes; /* scratch needed by emg_plan_build and emg_plan_order */
   int32_t record_bytes;   /* 8 (default) or 4: bytes per contribution record of the packed gather */
+  int32_t value_layout;   /* EMG_LAYOUT_PACKED (default) or EMG_LAYOUT_BLOCK: the element values
+                             emg_assemble writes and its gather reads */
+  size_t off_hoff;        /* block layout: uint16 list start per row pair of every chunk */
 } emg_plan;
 
 int emg_version(void);
@@ -156,6 +167,16 @@ int emg_plan_init(int64_t n_tets, int64_t n_assy, int64_t n_edges, int64_t n_tri
  * for every form. Values are identical either way. Updates plan_bytes. No
  * counterpart in the reference. */
 int emg_plan_set_record_width(emg_plan *plan, int bytes);
+
+/* Host-only, between emg_plan_init and emg_plan_build: the element-value
+ * layout of emg_assemble and of the plan's gather lists. EMG_LAYOUT_PACKED
+ * (default): the canonical upper triangle, one record per (row, column pair)
+ * contribution (record_bytes wide). EMG_LAYOUT_BLOCK: entity-pair blocks, one
+ * 4-byte record per (row pair, column pair) contribution -- the two rows and
+ * two columns of an entity pair come from the same tets, so one record and
+ * one contiguous read give four entries of A. A is bit for bit the same in
+ * both layouts. Updates plan_bytes. No counterpart in the reference. */
+int emg_plan_set_value_layout(emg_plan *plan, int layout);
 
 /* Builds the entity->tet incidence lists, column lengths and indptr[N+1]
  * (int32) on the device, then synchronises `stream` and stores nnz/max_col in
@@ -244,11 +265,11 @@ typedef struct {
 size_t emg_assemble_batch_table_bytes(int n_jobs);
 
 /* emg_assemble for n_jobs independent jobs in two launches: one element
- * kernel over all the jobs' tets, then one packed gather over all their
- * entity chunks (each CTA looks its job up in the table). Every job's A is
- * bit for bit what emg_assemble gives it alone. All jobs share one material
- * kind and the precision; their plans use 8-byte gather records. The table
- * is written to h_table (host, emg_assemble_batch_table_bytes) and copied to
+ * kernel over all the jobs' tets, then one gather over all their entity
+ * chunks (each CTA looks its job up in the table). Every job's A is bit for
+ * bit what emg_assemble gives it alone. All jobs share one material kind,
+ * the precision and the value layout (block plans, or packed ones with
+ * 8-byte gather records). The table is written to h_table (host, emg_assemble_batch_table_bytes) and copied to
  * d_table on the stream: when h_table is page-locked the copy is
  * asynchronous and h_table must stay untouched until the stream has passed
  * this call. No counterpart in the reference (batching of independent
@@ -263,7 +284,7 @@ int emg_assemble_batch(const emg_assembly_job *h_jobs, int n_jobs, int precision
  * call cudaMalloc/cudaFree, which synchronise the device). It has no
  * counterpart in the reference. The element-value scratch is a file-scope
  * device array of 96 MiB that every GPU loading this library holds until
- * exit: at most 29,959 assembled tets in EMG_FP64/EMG_EXACT, 59,918 in
+ * exit: at most 28,597 assembled tets in EMG_FP64/EMG_EXACT, 57,195 in
  * EMG_MIXED; larger plans return EMG_ERANGE. It calls no cudaMalloc/cudaFree.
  * Every call looks the array's address up in the current device's context
  * (cudaGetSymbolAddress), so a device reset between calls is safe; the

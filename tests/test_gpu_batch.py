@@ -24,11 +24,11 @@ def _cases():
     return [(a, None), (b, None), (d, cond)], [(c, None)]
 
 
-def _setup(cases, dev):
+def _setup(cases, dev, layout="block"):
     out = []
     for wl, cond in cases:
         dm = DeviceMesh(wl.field, cond, dev)
-        cm = GpuCSCMapping(dm)
+        cm = GpuCSCMapping(dm, value_layout=layout)
         mat = DeviceMaterial(wl.er, wl.ur, wl.n_tets, dev)
         out.append((wl, dm, cm, mat))
     return out
@@ -62,12 +62,13 @@ def _run_batch(items, precision, coefs, dev):
     return [A for _, A, _ in keep]
 
 
+@pytest.mark.parametrize("layout", ["block", "packed"])
 @pytest.mark.parametrize("precision", [L.EMG_FP64, L.EMG_MIXED, L.EMG_EXACT])
-def test_batch_equals_single_jobs(precision):
+def test_batch_equals_single_jobs(precision, layout):
     dev = torch.device("cuda", 0)
     iso, diag = _cases()
     for group in (iso, diag):
-        items = _setup(group, dev)
+        items = _setup(group, dev, layout)
         coefs = [(1.0 + 0.5j, -(3.0 + 0.25j) * (k + 1)) for k in range(len(items))]
         got = _run_batch(items, precision, coefs, dev)
         for (wl, dm, cm, mat), (a, b), A in zip(items, coefs, got):
@@ -82,6 +83,9 @@ def test_batch_rejects_mixed_kinds_and_small_tables():
     items = _setup([iso[0], diag[0]], dev)
     with pytest.raises(L.EmgError, match="material kind"):
         _run_batch(items, L.EMG_FP64, [(1.0, 0.0)] * 2, dev)
+    mixed_layouts = _setup([iso[0]], dev, "block") + _setup([iso[1]], dev, "packed")
+    with pytest.raises(L.EmgError, match="value layout"):
+        _run_batch(mixed_layouts, L.EMG_FP64, [(1.0, 0.0)] * 2, dev)
     descs = (L.AssemblyJobDesc * 1)()
     small = torch.empty(8, dtype=torch.uint8, pin_memory=True)
     assert L.lib().emg_assemble_batch(descs, 1, L.EMG_FP64, L.ptr(small), L.ptr(small), 8,

@@ -136,16 +136,18 @@ def test_mapping_rejects_other_mesh():
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_chunk_order_changes_no_value(mid_case, precision):
     """The Morton processing order of the gather's entity chunks and the
-    default interleave, with 8- or 4-byte contribution records, give bitwise
-    identical A (same sums, other warps)."""
+    default interleave, in the block layout and in the packed one with 8- or
+    4-byte contribution records, give bitwise identical A (same sums, other
+    warps)."""
     f, er, ur = mid_case[0], mid_case[1], mid_case[2]
     from emerge_b200.assembly import DeviceMaterial, DeviceMesh, _Job, _prec
 
     dm = DeviceMesh(f, np.zeros(0, np.int64))
     job = _Job(dm, DeviceMaterial(er, ur, dm.n_tets, dm.device), _prec(precision))
     outs = []
-    for order, width in (("interleave", 8), ("morton", 8), ("morton", 4), ("interleave", 4)):
-        cm = GpuCSCMapping(dm, chunk_order=order, record_bytes=width)
+    for order, width, layout in (("interleave", 8, "block"), ("morton", 8, "block"), ("morton", 8, "packed"),
+                                 ("interleave", 8, "packed"), ("morton", 4, "packed"), ("interleave", 4, "packed")):
+        cm = GpuCSCMapping(dm, chunk_order=order, record_bytes=width, value_layout=layout)
         outs.append(cm.assemble_device(job, 1.0 + 0j, -2345.5 + 1.25j)[: cm.nnz].cpu().numpy())
         dm.check_status()
     for o in outs[1:]:

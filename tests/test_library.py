@@ -37,8 +37,14 @@ def test_host_only_entry_points():
     assert lib.emg_plan_set_record_width(ctypes.byref(p), 4) == 0 and p.record_bytes == 4
     assert p.plan_bytes < wide
     assert lib.emg_plan_set_record_width(ctypes.byref(p), 3) == L.EMG_EINVAL
-    assert lib.emg_assemble_workspace_size(10, L.EMG_FP64) == 10 * 210 * 16
-    assert lib.emg_assemble_workspace_size(10, L.EMG_MIXED) == 10 * 210 * 8
+    # enough for either element-value layout (210 packed / 220 block values per tet)
+    assert lib.emg_assemble_workspace_size(10, L.EMG_FP64) == 10 * 220 * 16
+    assert lib.emg_assemble_workspace_size(10, L.EMG_MIXED) == 10 * 220 * 8
+    assert p.value_layout == L.EMG_LAYOUT_PACKED
+    packed = p.plan_bytes
+    assert lib.emg_plan_set_value_layout(ctypes.byref(p), L.EMG_LAYOUT_BLOCK) == 0
+    assert p.value_layout == L.EMG_LAYOUT_BLOCK and p.plan_bytes < packed
+    assert lib.emg_plan_set_value_layout(ctypes.byref(p), L.EMG_LAYOUT_COO) == L.EMG_EINVAL
 
 
 def test_size_limits_are_range_errors():

@@ -74,7 +74,7 @@ def test_noalloc_second_mesh_after_first():
 def test_noalloc_rejects_plans_beyond_its_scratch():
     lib = L.lib()
     plan = L.Plan()
-    L.check(lib.emg_plan_init(40000, 40000, 48000, 80000, ctypes.byref(plan)))  # 40,000 tets > 29,959
+    L.check(lib.emg_plan_init(40000, 40000, 48000, 80000, ctypes.byref(plan)))  # 40,000 tets > 28,597
     mat = L.Material(L.EMG_MAT_ISO, None, None)
     rc = lib.emg_assemble_noalloc(ctypes.byref(plan), None, None, None, 0, None, None, ctypes.byref(mat), L.EMG_FP64,
                                   1.0, 0.0, 0.0, 0.0, None, None, None)
