@@ -811,8 +811,17 @@ __device__ __forceinline__ void element_cta(const ElemArgs &a, int64_t ia0, unsi
   }
 }
 
+// CTAs per SM the compiler must fit: the mixed isotropic form at 168
+// registers (three CTAs, 48 bytes of spills) measured 21% faster than at 235
+// (two); the FP64 forms, the mixed 4-CTA cap (128 registers) and the mixed
+// diagonal form at three CTAs measured slower.
+template <int FORM, int KIND>
+constexpr int elem_min_blocks() {
+  return (FORM == FORM_REF32 && KIND == EMG_MAT_ISO) ? 3 : 1;
+}
+
 template <int FORM, int KIND, int LAYOUT>
-__global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
+__global__ void __launch_bounds__(ELEM_THREADS, elem_min_blocks<FORM, KIND>()) k_element(ElemArgs a) {
   extern __shared__ __align__(16) unsigned char stage_raw[];
   element_cta<FORM, KIND, LAYOUT>(a, (int64_t)blockIdx.x * ELEM_THREADS, stage_raw);
 }
@@ -821,8 +830,8 @@ __global__ void __launch_bounds__(ELEM_THREADS) k_element(ElemArgs a) {
 // the packed form: job j owns the CTAs [cta_start[j], cta_start[j + 1]) and
 // its tets in CTA order, as if launched alone.
 template <int FORM, int KIND, int LAYOUT>
-__global__ void __launch_bounds__(ELEM_THREADS) k_element_batch(const ElemArgs *jobs, const int64_t *cta_start,
-                                                                int n_jobs) {
+__global__ void __launch_bounds__(ELEM_THREADS, elem_min_blocks<FORM, KIND>())
+    k_element_batch(const ElemArgs *jobs, const int64_t *cta_start, int n_jobs) {
   extern __shared__ __align__(16) unsigned char stage_raw[];
   const int64_t b = blockIdx.x;
   int lo = 0, hi = n_jobs - 1;  // the job with cta_start[j] <= b < cta_start[j + 1]

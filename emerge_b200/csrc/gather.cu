@@ -253,10 +253,15 @@ __device__ __forceinline__ void gather_block_chunk(const ChunkMeta &m, const uin
   const int64_t hb = m.hbase / 2;
   int e = 0;
   // list bounds of the lane's next row pair are loaded while the current one is summed
+  // complex64 values: the first record of the lane's next row pair is also
+  // loaded ahead (measured 2% faster; slower for complex128)
+  constexpr bool RECORD_AHEAD = !std::is_same<R, double>::value;
   int n0 = 0, n1 = 0;
+  uint32_t r0n = 0;
   if (lane < H) {
     n0 = hoff[hb + lane];
     n1 = lane + 1 < H ? (int)hoff[hb + lane + 1] : total;
+    if (RECORD_AHEAD && n0 < min(n1, total)) r0n = __ldg(rl + n0);
   }
   for (int h = lane; h < H; h += 32) {
     while (e + 1 < m.nx && h >= hs[e + 1]) ++e;  // h only grows along a lane
@@ -266,13 +271,14 @@ __device__ __forceinline__ void gather_block_chunk(const ChunkMeta &m, const uin
     const int pp = hl < ne ? p + ne : p + nf;
     const int o0 = n0;
     const int o1 = min(n1, total);
+    const uint32_t r0 = r0n;
     if (h + 32 < H) {
       n0 = hoff[hb + h + 32];
       n1 = h + 33 < H ? (int)hoff[hb + h + 33] : total;
     }
     double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0, s2r = 0.0, s2i = 0.0, s3r = 0.0, s3i = 0.0;
     for (int k = o0; k < o1; ++k) {
-      const uint32_t rec = __ldg(rl + k);
+      const uint32_t rec = (RECORD_AHEAD && k == o0) ? r0 : __ldg(rl + k);
       const int64_t b = rec & 0x7fffffffu;
       if (b >= n_blocks) continue;  // only a plan whose build was flagged can hold this
       const C64 u0 = load_val<R>(v, 4 * b), u3 = load_val<R>(v, 4 * b + 3);
@@ -291,6 +297,7 @@ __device__ __forceinline__ void gather_block_chunk(const ChunkMeta &m, const uin
       s3r += u3.re;
       s3i += u3.im;
     }
+    if (RECORD_AHEAD && h + 32 < H && n0 < min(n1, total)) r0n = __ldg(rl + n0);
     A[m.A0 + p] = make_double2(ar * s0r - ai * s0i, ar * s0i + ai * s0r);
     A[m.A1 + p] = make_double2(ar * s1r - ai * s1i, ar * s1i + ai * s1r);
     A[m.A0 + pp] = make_double2(ar * s2r - ai * s2i, ar * s2i + ai * s2r);
