@@ -12,9 +12,14 @@
 //    moments mu[alpha] = sum_q w_q L~_q^alpha (degree <= 4) contracted with
 //    the tensors G = V (eps grad L~_m).grad L~_n and H = V (mu^-1 X_P).X_Q
 //    through generated tables (nedelec_moment_tables.cuh).
-//  FORM_REF32 (EMG_MIXED): the same FP64 geometry and L~; the quadrature
-//    products (moments), tensors and their contraction in FP32 with FP32
-//    accumulation; element values complex64.
+//  FORM_REF32 (EMG_MIXED): FP64 geometry from edge vectors (Jacobian,
+//    determinant, gradients, orientation sign), the tensors G and H formed in
+//    FP64 and rounded to FP32, then contracted in FP32 with FP32 accumulation
+//    against the closed-form tables (nedelec_tables.cuh). KEAST4 integrates
+//    every product of two basis values or curls of this element exactly, so
+//    its 11-point sums are fixed rational combinations of the tensors; the
+//    tables hold them, evaluated once when the tables are generated. Element
+//    values complex64.
 //  FORM_EXACT (EMG_EXACT): exact closed-form integrals (nedelec_tables.cuh)
 //    on accurate edge-vector geometry, free of the reference's cancellation.
 //
@@ -492,7 +497,7 @@ __device__ __forceinline__ void entry(const Tensors<KIND, R> &T, const R *mu, do
                                       typename EntryT<KIND, R>::T &k, typename EntryT<KIND, R>::T &m) {
   using E = typename EntryT<KIND, R>::T;
   E ak{}, am{};
-  if constexpr (FORM == FORM_EXACT) {
+  if constexpr (FORM != FORM_REF64) {
     emg_tables::Pair<f, s>::stiff(ak, T.H);
     emg_tables::Pair<f, s>::mass(am, T.G);
     if (emg_tables::odd(f) != emg_tables::odd(s)) {
@@ -736,7 +741,7 @@ __device__ __forceinline__ void element_cta(const ElemArgs &a, int64_t ia0, unsi
   const int ia = (int)ia64;
   Geo G;
   Tensors<KIND, R> T;
-  R mu[FORM == FORM_EXACT ? 1 : NMOM];
+  R mu[FORM == FORM_REF64 ? NMOM : 1];
   CR<R> cK{0, 0}, cM{0, 0};
   double sig = 1.0;
   uint64_t inv = 0;
@@ -761,7 +766,7 @@ __device__ __forceinline__ void element_cta(const ElemArgs &a, int64_t ia0, unsi
 #pragma unroll
         for (int d = 0; d < 3; ++d) X[d][q] = a.nodes[(int64_t)d * a.nN + v[q]];
       bool good;
-      if constexpr (FORM == FORM_EXACT) {
+      if constexpr (FORM != FORM_REF64) {
         good = exact_geometry(X, v, G);
       } else {
         good = ref_geometry<R>(X, v, G, mu);
@@ -811,13 +816,14 @@ __device__ __forceinline__ void element_cta(const ElemArgs &a, int64_t ia0, unsi
   }
 }
 
-// CTAs per SM the compiler must fit: the mixed isotropic form at 168
-// registers (three CTAs, 48 bytes of spills) measured 21% faster than at 235
-// (two); the FP64 forms, the mixed 4-CTA cap (128 registers) and the mixed
-// diagonal form at three CTAs measured slower.
+// CTAs per SM the compiler must fit. Measured on the 2.01M-tet box: the
+// FP64 forms at their natural 242-255 registers (two CTAs) beat every cap (a
+// three-CTA cap: 1.84 -> 3.68 ms, 1.9 KB of spills); the mixed form needs 88-254
+// registers with no cap (five CTAs per SM for the isotropic instance, set by
+// its 42 KB stage as much as by registers).
 template <int FORM, int KIND>
 constexpr int elem_min_blocks() {
-  return (FORM == FORM_REF32 && KIND == EMG_MAT_ISO) ? 3 : 1;
+  return 1;
 }
 
 template <int FORM, int KIND, int LAYOUT>

@@ -68,9 +68,12 @@ enum {
                     coordinate barycentric coefficients, KEAST4 points and
                     barycentric values, unfused), quadrature sums evaluated
                     as per-tet moments; element values complex128 */
-  EMG_MIXED = 1, /* FP64 geometry/orientation/determinant/barycentric values
-                    and final sum; FP32 quadrature products, accumulation
-                    and contraction; element values complex64 */
+  EMG_MIXED = 1, /* FP64 geometry (edge vectors, determinant, gradients,
+                    orientation sign), FP64 tensors rounded to FP32 and
+                    contracted in FP32 with FP32 accumulation against the
+                    11-point rule's sums of basis products (exact for this
+                    element, so precomputed); FP64 final sum; element
+                    values complex64 */
   EMG_EXACT = 2, /* exact closed-form integrals on edge-vector geometry in
                     FP64 (free of the reference's cancellation error, so it
                     differs from the reference by that error); complex128 */
