@@ -18,8 +18,10 @@ Differences from the reference, on purpose:
 * a zero-volume, non-finite or index-invalid tet raises ``EmgMeshError``
   (the reference silently produces inf/NaN entries);
 * ``precision="fp64"`` (default) reproduces the reference's own FP64
-  arithmetic; ``"mixed"`` runs the quadrature products in FP32 (relative
-  error <= 1e-6 against FP64); ``"exact"`` evaluates the element integrals
+  arithmetic; ``"mixed"`` keeps the geometry in FP64 and contracts the
+  quadrature's (exact, precomputed) sums of basis products with the tet's
+  tensors in FP32 (relative error <= 1e-6 against FP64, and closer than
+  FP64 to the exact integrals on sliver tets); ``"exact"`` evaluates the element integrals
   in closed form, free of the reference's absolute-coordinate cancellation
   (it then differs from the reference by the reference's rounding error).
 """
