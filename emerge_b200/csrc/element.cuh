@@ -23,9 +23,11 @@
 //  FORM_EXACT (EMG_EXACT): exact closed-form integrals (nedelec_tables.cuh)
 //    on accurate edge-vector geometry, free of the reference's cancellation.
 //
-// Every form writes the reference's COO layout value[ia*400 + 20*a + b]: one
-// 20-value row of the block at a time is staged in shared memory and the warp
-// writes its 32 rows as contiguous 320-byte (160-byte) runs.
+// Every form writes one of three layouts (element_cta): the reference's COO
+// block value[ia*400 + 20*a + b], the packed canonical upper triangle
+// [ia][210], or the entity-pair blocks [ia][220] of the assembly path. One row
+// of the block at a time is staged in shared memory and the warp writes its
+// 32 tets' rows as contiguous runs.
 #pragma once
 #include "common.cuh"
 
