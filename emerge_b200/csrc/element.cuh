@@ -649,14 +649,15 @@ __device__ __forceinline__ void do_row_packed(const Tensors<KIND, R> &T, const R
   if (active)
     compute_row_packed<X, FORM, KIND, R>(T, mu, sig, cK, cM, inv, stage + lane * (W | 1),
                                          std::make_integer_sequence<int, W>{});
+  // the warp's 32 tets are consecutive assembled indices: lane r's is ia - lane + r
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  const int64_t ia_w = (int64_t)ia - lane;
   __syncwarp();
 #pragma unroll 1
   for (int it = 0; it < W; ++it) {
     const int e = it * 32 + lane;
     const int r = e / W, c = e - r * W;
-    const int ia_r = __shfl_sync(0xffffffffu, ia, r);
-    const bool act_r = __shfl_sync(0xffffffffu, (int)active, r);
-    if (act_r) out[(int64_t)ia_r * 210 + packed_index(X, X) + c] = stage[r * (W | 1) + c];
+    if ((act >> r) & 1u) out[(ia_w + r) * 210 + packed_index(X, X) + c] = stage[r * (W | 1) + c];
   }
   __syncwarp();
 }
@@ -702,14 +703,15 @@ __device__ __forceinline__ void do_row_block(const Tensors<KIND, R> &T, const R 
   if (active)
     compute_block_row<I, FORM, KIND, R>(T, mu, sig, cK, cM, inv, stage + lane * (W | 1),
                                         std::make_integer_sequence<int, 10 - I>{});
+  // the warp's 32 tets are consecutive assembled indices: lane r's is ia - lane + r
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  const int64_t ia_w = (int64_t)ia - lane;
   __syncwarp();
 #pragma unroll 1
   for (int it = 0; it < W; ++it) {
     const int e = it * 32 + lane;
     const int r = e / W, c = e - r * W;
-    const int ia_r = __shfl_sync(0xffffffffu, ia, r);
-    const bool act_r = __shfl_sync(0xffffffffu, (int)active, r);
-    if (act_r) out[(int64_t)ia_r * kBlockValues + 4 * block_index(I, I) + c] = stage[r * (W | 1) + c];
+    if ((act >> r) & 1u) out[(ia_w + r) * kBlockValues + 4 * block_index(I, I) + c] = stage[r * (W | 1) + c];
   }
   __syncwarp();
 }
