@@ -653,7 +653,7 @@ __device__ __forceinline__ void do_row_packed(const Tensors<KIND, R> &T, const R
   const unsigned act = __ballot_sync(0xffffffffu, active);
   const int64_t ia_w = (int64_t)ia - lane;
   __syncwarp();
-#pragma unroll 1
+#pragma unroll 2
   for (int it = 0; it < W; ++it) {
     const int e = it * 32 + lane;
     const int r = e / W, c = e - r * W;
@@ -707,7 +707,7 @@ __device__ __forceinline__ void do_row_block(const Tensors<KIND, R> &T, const R 
   const unsigned act = __ballot_sync(0xffffffffu, active);
   const int64_t ia_w = (int64_t)ia - lane;
   __syncwarp();
-#pragma unroll 1
+#pragma unroll 2
   for (int it = 0; it < W; ++it) {
     const int e = it * 32 + lane;
     const int r = e / W, c = e - r * W;
